@@ -1,0 +1,137 @@
+/*
+ * rpb200.h -- C ABI of the REAPERS B200 hot path (librpb200.so).
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success or a
+ * negative status (RP_E_*); rp_last_error() returns the message of the last
+ * failure on the calling thread.  Vectors are device pointers to interleaved
+ * complex numbers (RP_C64: float re/im, 8 bytes; RP_C128: double re/im, 16
+ * bytes), 16-byte aligned, of length 2^len.  All calls are ordered on the
+ * library's stream (rp_stream()); calls that return a scalar or copy to the
+ * host synchronise it, matching the synchronous semantics of the reference's
+ * GPUImpl (inc/gpuimpl.h:628-638).
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * cl91/REAPERS).
+ */
+#ifndef RPB200_H
+#define RPB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RP_C64 1  /* complex<float>  */
+#define RP_C128 2 /* complex<double> */
+
+#define RP_OK 0
+#define RP_E_INTERNAL -1
+#define RP_E_INVALID -2   /* InvalidArgument (inc/except.h:101-118) */
+#define RP_E_CUDA -3      /* CudaError (inc/except.h:131-140) */
+#define RP_E_NOMEM -4     /* DevOutOfMem (inc/except.h:162-170) */
+#define RP_E_DEVICE -5    /* a device-side wait gave up (kernel error word) */
+#define RP_E_NODEVICE -6  /* NoGpuDevice (inc/except.h:143-149) */
+
+typedef struct rp_ham *rp_ham_t;
+
+/* Per-Hamiltonian plan of the H.psi kernel. */
+typedef struct {
+    int len;             /* spin chain length */
+    int dtype;           /* RP_C64 or RP_C128 */
+    int nterms;          /* Pauli strings */
+    int tile_exp;        /* B: output tile of 2^B elements (0: direct kernel) */
+    int ngroups;         /* distinct high X-mask parts x >> B */
+    int threads;         /* consumer threads per CTA */
+    int stages;          /* shared-memory pipeline depth */
+    int grid;            /* persistent CTAs */
+    double alg_bytes;    /* (ngroups + 1) * 2^len * element size per apply */
+} rp_ham_info_t;
+
+/* Statistics of one evolve. */
+typedef struct {
+    int restarts;        /* Arnoldi cycles */
+    int applies;         /* H.psi products */
+    int passes;          /* orthogonalisation passes */
+    int prods;           /* inner products the reference's MGS would take */
+    int breakdown;       /* 1 if an invariant subspace ended the evolve */
+    double last_err;     /* ||Hexp0|| of the final cycle */
+} rp_evolve_stats_t;
+
+/* --- context ------------------------------------------------------------ */
+/* Select the device and create the stream.  Replaces the static-init
+ * GPUContext (inc/gpuimpl.h:496-559); called lazily by every entry point. */
+int rp_init(int device);
+/* Release cached workspaces and the stream. */
+int rp_shutdown(void);
+const char *rp_last_error(void);
+/* GPUImpl::get_device_count (inc/gpuimpl.h:590-592). */
+int rp_device_count(int *count);
+/* The cudaStream_t all calls are ordered on. */
+void *rp_stream(void);
+int rp_synchronize(void);
+
+/* --- memory (DeviceVec, inc/gpuimpl.h:405-494) -------------------------- */
+int rp_alloc(void **ptr, size_t bytes);
+int rp_free(void *ptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device. */
+int rp_memcpy(void *dst, const void *src, size_t bytes, int kind);
+
+/* --- vector operations (GPUImpl BLAS-1, inc/gpuimpl.h:853-1002) -------- */
+/* GPUImpl::zero_vec */
+int rp_vec_zero(int dtype, uint64_t n, void *v);
+/* GPUImpl::copy_vec, same precision and float<->double (rounds to nearest,
+ * as CPUImpl::copy_vec does; the reference GPU kernel krnl_dtof_vec rounds
+ * toward zero, src/krnl.cu:31-39) */
+int rp_vec_copy(int dtype_dst, void *dst, int dtype_src, const void *src, uint64_t n);
+/* GPUImpl::add_vec(v0, s, v1): y += (ar + i ai) x */
+int rp_vec_axpy(int dtype, uint64_t n, void *y, double ar, double ai, const void *x);
+/* GPUImpl::add_vec(res, v0, v1): res = a + b */
+int rp_vec_add(int dtype, uint64_t n, void *res, const void *a, const void *b);
+/* GPUImpl::scale_vec: v *= (ar + i ai) */
+int rp_vec_scale(int dtype, uint64_t n, void *v, double ar, double ai);
+/* GPUImpl::vec_prod: out[0] + i out[1] = <a|b> (conjugate-linear in a),
+ * FP64 compensated accumulation */
+int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out);
+/* GPUImpl::vec_norm */
+int rp_vec_norm(int dtype, uint64_t n, const void *v, double *out);
+/* GPUImpl::init_random without the normalisation: i.i.d. complex Gaussian
+ * entries from a counter-based generator (deterministic per seed). */
+int rp_vec_random(int dtype, uint64_t n, void *v, uint64_t seed);
+
+/* --- Hamiltonian (DevSumOps, inc/gpuimpl.h:124-397, upload :1065-1085) -- */
+/* terms: bits[k] in SpinOp's encoding (bit 2i = X on site i, bit 2i+1 = Z,
+ * sigma_y stored as X|Z with the factor i in the coefficient, inc/ops.h:
+ * 138-143, 285-288); coeff[2k], coeff[2k+1] = stored coefficient.  Equal
+ * bit strings are summed by the caller (HostSumOps::operator+=,
+ * inc/cpuimpl.h:233-253).  The table is grouped for the kernel here. */
+int rp_ham_create(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                  const double *coeff);
+/* Same with an explicit tile exponent (5..12; 0 = default), for tuning. */
+int rp_ham_create_ex(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                     const double *coeff, int tile_exp);
+int rp_ham_destroy(rp_ham_t h);
+int rp_ham_info(rp_ham_t h, rp_ham_info_t *info);
+
+/* --- hot path ------------------------------------------------------------ */
+/* GPUImpl::apply_ops (src/krnl.cu:220-257): out = H in, or out += H in when
+ * accumulate != 0.  in and out must differ. */
+int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
+
+/* Krylov<Impl>::evolve (inc/algo.h:267-365) as called by State::evolve
+ * (inc/state.h:415-424): psi <- exp(-(beta + i t) H) psi in place, restarted
+ * Arnoldi with krydim basis vectors, stop when ||Hexp0|| < tol, on breakdown,
+ * or after max_iters restarts (0 = no limit).  t == 0 and beta == 0 returns
+ * immediately, as State::evolve does.  stats may be NULL. */
+int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double tol,
+              int max_iters, rp_evolve_stats_t *stats);
+
+/* Free the cached Krylov workspace (krydim + 2 vectors). */
+int rp_workspace_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RPB200_H */

@@ -1,0 +1,198 @@
+"""REAPERS hot path on B200: Pauli-sum H.psi and restarted Krylov exp(-iHt)psi.
+
+Python host layer over the C ABI of ``librpb200.so`` (include/rpb200.h).
+State vectors are CUDA tensors (complex64 / complex128, contiguous); the
+library reads and writes them in place through their device pointers.  The
+operations mirror the reference's backend concept (inc/gpuimpl.h:853-1047)
+and ``State::evolve`` (inc/state.h:415-424).  There is no CPU fallback: every
+call goes to the CUDA kernels and raises if the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import RP_C64, RP_C128, RPError
+from . import syk  # noqa: F401  (term generators)
+
+__all__ = ["Hamiltonian", "evolve", "dot", "norm", "axpy", "scale", "random_state",
+           "stream", "synchronize", "RPError", "RP_C64", "RP_C128", "dtype_code", "syk",
+           "otoc"]
+
+
+def dtype_code(dtype):
+    """'c64'/'c128'/torch dtype/numpy dtype -> RP_C64 / RP_C128."""
+    s = str(dtype)
+    if s in ("c64", "complex64", "torch.complex64", "1"):
+        return RP_C64
+    if s in ("c128", "complex128", "torch.complex128", "2"):
+        return RP_C128
+    raise ValueError(f"unsupported dtype {dtype!r}")
+
+
+def _ptr(t):
+    """Device pointer of a contiguous CUDA tensor (or a raw integer pointer)."""
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    if not t.is_cuda:
+        raise ValueError("vector must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("vector must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def _tcode(t):
+    import torch
+    if t.dtype == torch.complex64:
+        return RP_C64
+    if t.dtype == torch.complex128:
+        return RP_C128
+    raise ValueError(f"vector dtype {t.dtype} is not complex64/complex128")
+
+
+def init(device=0):
+    _lib.call("rp_init", int(device))
+
+
+def stream():
+    """The library's CUDA stream as a torch.cuda.ExternalStream."""
+    import torch
+    return torch.cuda.ExternalStream(_lib.load().rp_stream())
+
+
+def synchronize():
+    _lib.call("rp_synchronize")
+
+
+class Hamiltonian:
+    """A sum of Pauli strings uploaded and grouped for the H.psi kernel.
+
+    bits: uint64 SpinOp bit strings (bit 2i = X on site i, bit 2i+1 = Z);
+    coeff: the stored complex coefficients (sigma_y carries its i here, as in
+    inc/ops.h:285-288).  Mirrors DevSumOps::upload (inc/gpuimpl.h:1065-1085).
+    """
+
+    def __init__(self, length, bits, coeff, dtype="c128", tile_exp=None):
+        self.len = int(length)
+        self.dtype = dtype_code(dtype)
+        b = np.ascontiguousarray(bits, dtype=np.uint64)
+        c = np.ascontiguousarray(coeff, dtype=np.complex128)
+        if b.shape != c.shape:
+            raise ValueError("bits and coeff must have the same length")
+        self.nterms = len(b)
+        cd = c.view(np.float64)
+        h = C.c_void_p()
+        _lib.call("rp_ham_create_ex", C.byref(h), self.len, self.dtype, self.nterms,
+                  b.ctypes.data_as(C.POINTER(C.c_uint64)),
+                  cd.ctypes.data_as(C.POINTER(C.c_double)), int(tile_exp or 0))
+        self._h = h
+        self.bits, self.coeff = b.copy(), c.copy()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        i = _lib.HamInfo()
+        _lib.call("rp_ham_info", self._h, C.byref(i))
+        return {k: getattr(i, k) for k, _ in _lib.HamInfo._fields_}
+
+    def apply(self, out, inp, accumulate=False):
+        """out = H inp (out += H inp with accumulate)."""
+        if _tcode(out) != self.dtype or _tcode(inp) != self.dtype:
+            raise ValueError("vector precision does not match the Hamiltonian's")
+        _lib.call("rp_apply", self._h, _ptr(out), _ptr(inp), 1 if accumulate else 0)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().rp_ham_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def evolve(ham, psi, t, beta=0.0, krydim=5, tol=None, max_iters=0):
+    """psi <- exp(-(beta + i t) H) psi in place (State::evolve, inc/state.h:415-424).
+
+    tol defaults to the machine epsilon of the state's precision, as
+    Krylov::evolve's default (inc/algo.h:267-269)."""
+    if _tcode(psi) != ham.dtype:
+        raise ValueError("state precision does not match the Hamiltonian's")
+    if tol is None:
+        tol = float(np.finfo(np.float32 if ham.dtype == RP_C64 else np.float64).eps)
+    st = _lib.EvolveStats()
+    _lib.call("rp_evolve", ham.handle, _ptr(psi), float(t), float(beta), int(krydim),
+              float(tol), int(max_iters), C.byref(st))
+    return {k: getattr(st, k) for k, _ in _lib.EvolveStats._fields_}
+
+
+def dot(a, b):
+    """<a|b> (GPUImpl::vec_prod), FP64 compensated."""
+    out = (C.c_double * 2)()
+    _lib.call("rp_vec_dot", _tcode(a), a.numel(), _ptr(a), _ptr(b), out)
+    return complex(out[0], out[1])
+
+
+def norm(v):
+    out = C.c_double()
+    _lib.call("rp_vec_norm", _tcode(v), v.numel(), _ptr(v), C.byref(out))
+    return out.value
+
+
+def axpy(y, a, x):
+    """y += a x."""
+    a = complex(a)
+    _lib.call("rp_vec_axpy", _tcode(y), y.numel(), _ptr(y), a.real, a.imag, _ptr(x))
+    return y
+
+
+def scale(v, a):
+    a = complex(a)
+    _lib.call("rp_vec_scale", _tcode(v), v.numel(), _ptr(v), a.real, a.imag)
+    return v
+
+
+def copy(dst, src):
+    _lib.call("rp_vec_copy", _tcode(dst), _ptr(dst), _tcode(src), _ptr(src), dst.numel())
+    return dst
+
+
+def random_state(length, dtype="c128", seed=0, normalize=True, device="cuda"):
+    """Complex Gaussian vector of 2^length entries made on the GPU (counter-based,
+    deterministic per seed), optionally normalised (GPUImpl::init_random)."""
+    import torch
+    code = dtype_code(dtype)
+    t = torch.empty(1 << length, dtype=torch.complex64 if code == RP_C64 else torch.complex128,
+                    device=device)
+    _lib.call("rp_vec_random", code, t.numel(), _ptr(t), int(seed))
+    if normalize:
+        scale(t, 1.0 / norm(t))
+    return t
+
+
+def otoc(ham, w, v, psi0, times, krydim=5, tol=None):
+    """F(t) = <psi0| W(t) V W(t) V |psi0> at beta = 0, in the operation order of
+    examples/simple-syk-krylov.cc:42-57 (psi = V psi0; e^{-iHt}; W; e^{iHt};
+    V; e^{-iHt}; W; e^{iHt}; <psi0|psi>).  w and v are Hamiltonian objects of
+    single Majorana strings.  Returns (values, total H.psi count)."""
+    import torch
+    vals = []
+    applies = 0
+    psi = torch.empty_like(psi0)
+    tmp = torch.empty_like(psi0)
+    for t in times:
+        v.apply(psi, psi0)
+        for op, tt in ((w, t), (v, -t), (w, t), (None, -t)):
+            applies += evolve(ham, psi, tt, 0.0, krydim, tol)["applies"]
+            if op is not None:
+                op.apply(tmp, psi)
+                psi, tmp = tmp, psi
+        vals.append(dot(psi0, psi))
+    return np.array(vals), applies

@@ -1,0 +1,342 @@
+// C ABI of librpb200.so: argument checking, error translation, context.
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/rpb200.h"
+#include "rp_apply.cuh"
+#include "rp_krylov.cuh"
+#include "rp_vec.cuh"
+
+struct rp_ham {
+    rp::ApplyPlan plan;
+};
+
+namespace rp {
+
+static thread_local std::string g_err = "no error";
+static cudaStream_t g_stream = nullptr;
+static int g_device = -1;
+static KryWorkspace g_ws;
+static std::mutex g_mu;
+
+void set_error(int code, const std::string &msg) {
+    (void)code;
+    g_err = msg;
+}
+
+static void ensure_init() {
+    if (g_stream) return;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) throw Error{RP_E_NODEVICE, "no CUDA device available"};
+    if (g_device < 0) g_device = 0;
+    RP_CUDA(cudaSetDevice(g_device));
+    RP_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+}
+
+static size_t esize(int dtype) { return dtype == RP_C128 ? 16 : 8; }
+
+static void check_dtype(int dtype) {
+    RP_REQUIRE(dtype == RP_C64 || dtype == RP_C128, RP_E_INVALID,
+               "dtype must be RP_C64 (1) or RP_C128 (2)");
+}
+
+static void check_vec(const void *p) {
+    RP_REQUIRE(p != nullptr, RP_E_INVALID, "null vector pointer");
+    RP_REQUIRE(((uintptr_t)p & 15) == 0, RP_E_INVALID, "vectors must be 16-byte aligned");
+}
+
+template <typename F>
+static int guarded(F &&f) {
+    try {
+        std::lock_guard<std::mutex> lk(g_mu);
+        ensure_init();
+        f();
+        return RP_OK;
+    } catch (const Error &e) {
+        set_error(e.code, e.msg);
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_error(RP_E_NOMEM, "host out of memory");
+        return RP_E_NOMEM;
+    } catch (const std::exception &e) {
+        set_error(RP_E_INTERNAL, e.what());
+        return RP_E_INTERNAL;
+    }
+}
+
+}  // namespace rp
+
+using namespace rp;
+
+extern "C" {
+
+int rp_init(int device) {
+    try {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (g_stream && device != g_device) {
+            throw Error{RP_E_INVALID, "rp_init: the library is already bound to another device"};
+        }
+        g_device = device;
+        ensure_init();
+        return RP_OK;
+    } catch (const Error &e) {
+        set_error(e.code, e.msg);
+        return e.code;
+    }
+}
+
+int rp_shutdown(void) {
+    try {
+        std::lock_guard<std::mutex> lk(g_mu);
+        workspace_release(g_ws);
+        if (g_stream) cudaStreamDestroy(g_stream);
+        g_stream = nullptr;
+        return RP_OK;
+    } catch (const Error &e) {
+        set_error(e.code, e.msg);
+        return e.code;
+    }
+}
+
+const char *rp_last_error(void) { return g_err.c_str(); }
+
+int rp_device_count(int *count) {
+    if (!count) {
+        set_error(RP_E_INVALID, "null output pointer");
+        return RP_E_INVALID;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    *count = n;
+    return RP_OK;
+}
+
+void *rp_stream(void) {
+    void *s = nullptr;
+    guarded([&] { s = (void *)g_stream; });
+    return s;
+}
+
+int rp_synchronize(void) {
+    return guarded([&] { RP_CUDA(cudaStreamSynchronize(g_stream)); });
+}
+
+int rp_alloc(void **ptr, size_t bytes) {
+    return guarded([&] {
+        RP_REQUIRE(ptr, RP_E_INVALID, "null output pointer");
+        *ptr = nullptr;
+        cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 16);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{RP_E_NOMEM, "failed to allocate " + std::to_string(bytes) +
+                                        " bytes on the GPU device"};
+        }
+    });
+}
+
+int rp_free(void *ptr) {
+    return guarded([&] {
+        if (ptr) {
+            RP_CUDA(cudaStreamSynchronize(g_stream));
+            RP_CUDA(cudaFree(ptr));
+        }
+    });
+}
+
+int rp_memcpy(void *dst, const void *src, size_t bytes, int kind) {
+    return guarded([&] {
+        RP_REQUIRE(kind >= 0 && kind <= 2, RP_E_INVALID, "kind must be 0, 1 or 2");
+        RP_REQUIRE(bytes == 0 || (dst && src), RP_E_INVALID, "null pointer");
+        const cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice
+                                           : (kind == 1 ? cudaMemcpyDeviceToHost
+                                                        : cudaMemcpyDeviceToDevice);
+        RP_CUDA(cudaMemcpyAsync(dst, src, bytes, k, g_stream));
+        if (kind != 2) RP_CUDA(cudaStreamSynchronize(g_stream));
+    });
+}
+
+int rp_vec_zero(int dtype, uint64_t n, void *v) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(v);
+        RP_CUDA(cudaMemsetAsync(v, 0, n * esize(dtype), g_stream));
+    });
+}
+
+int rp_vec_copy(int dtype_dst, void *dst, int dtype_src, const void *src, uint64_t n) {
+    return guarded([&] {
+        check_dtype(dtype_dst);
+        check_dtype(dtype_src);
+        check_vec(dst);
+        check_vec(src);
+        vec_convert(dtype_dst, dst, dtype_src, src, n, g_stream);
+    });
+}
+
+int rp_vec_axpy(int dtype, uint64_t n, void *y, double ar, double ai, const void *x) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(y);
+        check_vec(x);
+        vec_axpy(dtype, n, y, ar, ai, x, g_stream);
+    });
+}
+
+int rp_vec_add(int dtype, uint64_t n, void *res, const void *a, const void *b) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(res);
+        check_vec(a);
+        check_vec(b);
+        vec_add3(dtype, n, res, a, b, g_stream);
+    });
+}
+
+int rp_vec_scale(int dtype, uint64_t n, void *v, double ar, double ai) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(v);
+        vec_scale(dtype, n, v, ar, ai, g_stream);
+    });
+}
+
+int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(a);
+        check_vec(b);
+        RP_REQUIRE(out, RP_E_INVALID, "null output pointer");
+        static double *part = nullptr;
+        static double *red = nullptr;
+        const int g = reduce_grid();
+        if (!part) {
+            RP_CUDA(cudaMalloc((void **)&part, (size_t)g * 2 * sizeof(double)));
+            RP_CUDA(cudaMalloc((void **)&red, 2 * sizeof(double)));
+        }
+        VecTable tab{};
+        tab.p[0] = a;
+        multi_dot_partials(dtype, n, tab, 1, b, part, nullptr, nullptr, g_stream);
+        reduce_partials(part, g, 1, red, g_stream);
+        RP_CUDA(cudaMemcpyAsync(out, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, g_stream));
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+    });
+}
+
+int rp_vec_norm(int dtype, uint64_t n, const void *v, double *out) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(v);
+        RP_REQUIRE(out, RP_E_INVALID, "null output pointer");
+        *out = vec_norm_sync(dtype, n, v, nullptr, g_stream);
+    });
+}
+
+int rp_vec_random(int dtype, uint64_t n, void *v, uint64_t seed) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(v);
+        vec_random(dtype, n, v, seed, g_stream);
+    });
+}
+
+int rp_ham_create_ex(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                     const double *coeff, int tile_exp) {
+    return guarded([&] {
+        RP_REQUIRE(h, RP_E_INVALID, "null output pointer");
+        RP_REQUIRE(nterms == 0 || (bits && coeff), RP_E_INVALID, "null term table");
+        RP_REQUIRE(nterms < (1ull << 31), RP_E_INVALID, "too many terms");
+        check_dtype(dtype);
+        RP_REQUIRE(len >= 1 && len <= 32, RP_E_INVALID, "len must be in [1, 32]");
+        ApplyConfig cfg = default_config(len, dtype);
+        if (tile_exp) {
+            RP_REQUIRE(tile_exp >= 5 && tile_exp <= 12 && tile_exp <= len, RP_E_INVALID,
+                       "tile_exp must be in [5, min(12, len)]");
+            cfg.direct = false;
+            cfg.B = tile_exp;
+            cfg.P = std::min(256, 1 << tile_exp);
+        }
+        rp_ham *H = new rp_ham;
+        try {
+            plan_build(H->plan, len, dtype, bits, coeff, (int64_t)nterms, cfg);
+            plan_upload(H->plan);
+        } catch (...) {
+            plan_free(H->plan);
+            delete H;
+            throw;
+        }
+        *h = H;
+    });
+}
+
+int rp_ham_create(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                  const double *coeff) {
+    return rp_ham_create_ex(h, len, dtype, nterms, bits, coeff, 0);
+}
+
+int rp_ham_destroy(rp_ham_t h) {
+    return guarded([&] {
+        if (!h) return;
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+        plan_free(h->plan);
+        delete h;
+    });
+}
+
+int rp_ham_info(rp_ham_t h, rp_ham_info_t *info) {
+    return guarded([&] {
+        RP_REQUIRE(h && info, RP_E_INVALID, "null argument");
+        const ApplyPlan &p = h->plan;
+        info->len = p.len;
+        info->dtype = p.dtype;
+        info->nterms = p.nterms;
+        info->tile_exp = p.cfg.direct ? 0 : p.cfg.B;
+        info->ngroups = p.ngroups;
+        info->threads = p.cfg.direct ? 32 : p.cfg.P;
+        info->stages = p.cfg.direct ? 0 : p.cfg.stages;
+        info->grid = apply_grid(p);
+        info->alg_bytes = p.alg_bytes;
+    });
+}
+
+int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate) {
+    return guarded([&] {
+        RP_REQUIRE(h, RP_E_INVALID, "null Hamiltonian");
+        check_vec(out);
+        check_vec(in);
+        ApplyLaunch L;
+        L.in = in;
+        L.out = out;
+        L.accumulate = accumulate;
+        apply_launch(h->plan, L, g_stream);
+    });
+}
+
+int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double tol,
+              int max_iters, rp_evolve_stats_t *stats) {
+    return guarded([&] {
+        RP_REQUIRE(h, RP_E_INVALID, "null Hamiltonian");
+        check_vec(psi);
+        RP_REQUIRE(max_iters >= 0, RP_E_INVALID, "max_iters must be non-negative");
+        EvolveStats S{};
+        krylov_evolve(h->plan, g_ws, psi, t, beta, krydim, tol, max_iters, &S, g_stream);
+        if (stats) {
+            stats->restarts = S.restarts;
+            stats->applies = S.applies;
+            stats->passes = S.passes;
+            stats->prods = S.prods;
+            stats->breakdown = S.breakdown;
+            stats->last_err = S.last_err;
+        }
+    });
+}
+
+int rp_workspace_release(void) {
+    return guarded([&] {
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+        workspace_release(g_ws);
+    });
+}
+
+}  // extern "C"

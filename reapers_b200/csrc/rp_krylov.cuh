@@ -1,0 +1,69 @@
+// Restarted Krylov exp(-(beta + i t) H) psi on the GPU.
+#pragma once
+
+#include <vector>
+
+#include "rp_apply.cuh"
+#include "rp_vec.cuh"
+
+namespace rp {
+
+// Device-resident control state of one evolve.  Vectors u_i are stored
+// unnormalised; the Arnoldi basis is v_i = sigma[i] * u_i, so no separate
+// normalisation pass is ever made.
+struct KryDev {
+    int active;      // the current Arnoldi cycle is still running
+    int again;       // another orthogonalisation pass is due for this step
+    int niter;       // passes made for the current step
+    int m_eff;       // basis size of the cycle (krydim unless breakdown)
+    int brokedown;   // invariant subspace found
+    int passes;      // total orthogonalisation passes (statistics)
+    int prods;       // inner products the reference's MGS would take (statistics)
+    int pad;
+    double norm, old_norm, beta, oldbeta, beta0, nrm;
+    double sigma[MAX_KRYLOV + 1];
+    double hacc[2 * (MAX_KRYLOV + 1)];    // column j of H accumulated over passes
+    double coef[2 * (MAX_KRYLOV + 1)];    // update coefficients of the current pass
+    double ycoef[2 * (MAX_KRYLOV + 1)];   // beta0 * Hexp0_i * sigma_i
+    double H[2 * MAX_KRYLOV * MAX_KRYLOV];   // cycle Hessenberg matrix, column-major
+};
+
+struct EvolveStats {
+    int restarts;
+    int applies;
+    int passes;
+    int prods;
+    int breakdown;
+    double last_err;
+};
+
+// Workspace of one evolve: krydim+1 basis vectors, the answer, the device
+// state and the reduction buffers.
+struct KryWorkspace {
+    int len = 0, dtype = 0, krydim = 0;
+    uint64_t D = 0;
+    std::vector<void *> u;
+    void *y = nullptr;
+    KryDev *dev = nullptr;
+    double *partials = nullptr;
+    double *norm_partials = nullptr;
+    int hcap = 0;            // capacity (dimension) of Hfull
+    void *hfull = nullptr;   // hcap x hcap complex double
+    void *escratch = nullptr;
+    unsigned *err = nullptr;
+};
+
+void workspace_ensure(KryWorkspace &ws, int len, int dtype, int krydim);
+void workspace_release(KryWorkspace &ws);
+
+// psi <- exp(-(t_imag + i t_real) H) psi, restarted Arnoldi with the
+// Eiermann-Ernst update (inc/algo.h:267-365).  psi is a device vector of the
+// plan's precision.
+void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_real,
+                   double t_imag, int krydim, double tol, int max_iters, EvolveStats *stats,
+                   cudaStream_t st);
+
+// sqrt(<v|v>) (compensated FP64), synchronous.
+double vec_norm_sync(int dtype, uint64_t n, const void *v, KryWorkspace *ws, cudaStream_t st);
+
+}  // namespace rp

@@ -1,0 +1,185 @@
+"""GPU parity of the CUDA hot path against the CPU oracle (oracle/rp_oracle.c).
+
+Tolerances: FP64 (RP_C128) results within 1e-12 relative of the oracle --
+the bar the plain path is held to; integer work (indices, signs, operation
+counts) exact; FP32 (RP_C64) H.psi within 1e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+import reapers_b200 as rb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32_TOL = 1e-5
+
+
+def rand_terms(rng, L, T, kinds="mixed"):
+    bits = np.unique(rng.integers(0, 1 << (2 * L), size=T, dtype=np.uint64))
+    rng.shuffle(bits)
+    n = len(bits)
+    if kinds == "real":
+        coeff = rng.standard_normal(n) + 0j
+    elif kinds == "imag":
+        coeff = 1j * rng.standard_normal(n)
+    else:
+        coeff = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        coeff[::3] = coeff[::3].real
+        coeff[1::3] = 1j * coeff[1::3].imag
+    return bits, coeff
+
+
+def rand_vec(rng, L):
+    v = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    return v / np.linalg.norm(v)
+
+
+def to_dev(v, dtype):
+    t = torch.from_numpy(np.ascontiguousarray(v))
+    if dtype == "c64":
+        t = t.to(torch.complex64)
+    return t.cuda()
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6, 8, 10, 12, 14])
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_apply_random_terms(cuda, L, dtype):
+    rng = np.random.default_rng(100 + L)
+    bits, coeff = rand_terms(rng, L, 3 * L + 7)
+    v = rand_vec(rng, L)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    out = torch.empty(1 << L, dtype=torch.complex128 if dtype == "c128" else torch.complex64,
+                      device=cuda)
+    ham.apply(out, to_dev(v, dtype))
+    ref = O.apply(L, bits, coeff, v)
+    tol = FP64_TOL if dtype == "c128" else FP32_TOL
+    assert relerr(out.cpu().numpy().astype(np.complex128), ref) < tol
+
+
+@pytest.mark.parametrize("tile", [5, 6, 7, 8, 9, 10, 11, 12])
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_apply_every_tile_exponent(cuda, tile, dtype):
+    L = 13
+    rng = np.random.default_rng(tile)
+    bits, coeff = rand_terms(rng, L, 60)
+    v = rand_vec(rng, L)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype, tile_exp=tile)
+    assert ham.info()["tile_exp"] == tile
+    x = to_dev(v, dtype)
+    out = torch.empty_like(x)
+    ham.apply(out, x)
+    ref = O.apply(L, bits, coeff, v)
+    tol = FP64_TOL if dtype == "c128" else FP32_TOL
+    assert relerr(out.cpu().numpy().astype(np.complex128), ref) < tol
+    # accumulate: out += H x
+    ham.apply(out, x, accumulate=True)
+    assert relerr(out.cpu().numpy().astype(np.complex128), 2 * ref) < tol
+
+
+def test_apply_sparse_syk_and_identity(cuda):
+    N, L = 32, 16
+    bits, coeff = rb.syk.sparse_syk(N, k=8, seed=11)
+    # add an identity term and a pure-Z term (diagonal, group xh = 0)
+    bits = np.concatenate([bits, np.array([0, 2 << 8], np.uint64)])
+    coeff = np.concatenate([coeff, np.array([0.3, -0.7j])])
+    rng = np.random.default_rng(5)
+    v = rand_vec(rng, L)
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    out = torch.empty(1 << L, dtype=torch.complex128, device=cuda)
+    ham.apply(out, to_dev(v, "c128"))
+    assert relerr(out.cpu().numpy(), O.apply(L, bits, coeff, v)) < FP64_TOL
+
+
+def test_apply_empty_hamiltonian(cuda):
+    ham = rb.Hamiltonian(8, np.zeros(0, np.uint64), np.zeros(0, np.complex128), "c128")
+    x = to_dev(rand_vec(np.random.default_rng(0), 8), "c128")
+    out = torch.ones_like(x)
+    ham.apply(out, x)
+    assert torch.count_nonzero(out).item() == 0
+
+
+def test_apply_rejects_bad_arguments(cuda):
+    with pytest.raises(rb.RPError):
+        rb.Hamiltonian(4, np.array([1 << 10], np.uint64), np.array([1.0 + 0j]), "c128")
+    ham = rb.Hamiltonian(6, np.array([1], np.uint64), np.array([1.0 + 0j]), "c128")
+    x = torch.zeros(64, dtype=torch.complex128, device=cuda)
+    with pytest.raises(rb.RPError):
+        ham.apply(x, x)
+
+
+@pytest.mark.parametrize("L,N,k,t,beta,m", [
+    (8, 16, 0, 0.7, 0.0, 6), (10, 20, 4, 2.0, 0.0, 10), (10, 20, 4, -1.5, 0.3, 8),
+    (12, 24, 8, 5.0, 0.0, 20), (6, 12, 0, 3.0, 0.5, 5)])
+def test_evolve_fp64_matches_oracle(cuda, L, N, k, t, beta, m):
+    bits, coeff = rb.syk.sparse_syk(N, k=k, seed=L) if k else rb.syk.dense_syk(N, seed=L)
+    v = rand_vec(np.random.default_rng(L), L)
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    x = to_dev(v, "c128")
+    st = rb.evolve(ham, x, t, beta, m, 1e-12)
+    ref, st2 = O.evolve(L, bits, coeff, v, t, beta, m, 1e-12)
+    assert relerr(x.cpu().numpy(), ref) < FP64_TOL
+    for key in ("restarts", "applies", "passes", "prods", "breakdown"):
+        assert st[key] == st2[key], (key, st, st2)
+
+
+def test_evolve_fp32_mixed_precision(cuda):
+    L, N = 12, 24
+    bits, coeff = rb.syk.sparse_syk(N, k=8, seed=2)
+    v = rand_vec(np.random.default_rng(9), L)
+    ham = rb.Hamiltonian(L, bits, coeff, "c64")
+    x = to_dev(v, "c64")
+    rb.evolve(ham, x, 3.0, 0.0, 16, 1e-7)
+    ref, _ = O.evolve(L, bits, coeff, v, 3.0, 0.0, 16, 1e-12)
+    assert relerr(x.cpu().numpy().astype(np.complex128), ref) < 2e-5
+
+
+def test_evolve_breakdown_on_invariant_subspace(cuda):
+    # diagonal H on a basis state: H v = E v, breakdown at the first step
+    L = 6
+    bits = np.array([2 << 0, 2 << 2], np.uint64)   # sz(0) + sz(1)
+    coeff = np.array([0.4, -1.1 + 0j])
+    v = np.zeros(1 << L, np.complex128)
+    v[5] = 1.0
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    x = to_dev(v, "c128")
+    st = rb.evolve(ham, x, 1.3, 0.0, 5, 1e-12)
+    ref, st2 = O.evolve(L, bits, coeff, v, 1.3, 0.0, 5, 1e-12)
+    assert st["breakdown"] == st2["breakdown"] == 1
+    assert relerr(x.cpu().numpy(), ref) < FP64_TOL
+
+
+def test_evolve_zero_time_is_identity(cuda):
+    L = 8
+    bits, coeff = rb.syk.dense_syk(16, seed=1)
+    v = rand_vec(np.random.default_rng(1), L)
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    x = to_dev(v, "c128")
+    st = rb.evolve(ham, x, 0.0, 0.0, 5)
+    assert st["applies"] == 0
+    assert np.array_equal(x.cpu().numpy(), v)
+
+
+def test_vector_ops(cuda):
+    rng = np.random.default_rng(4)
+    a, b = rand_vec(rng, 14), rand_vec(rng, 14)
+    ta, tb = to_dev(a, "c128"), to_dev(b, "c128")
+    assert abs(rb.dot(ta, tb) - np.vdot(a, b)) < 1e-14
+    assert abs(rb.norm(ta) - np.linalg.norm(a)) < 1e-14
+    rb.axpy(ta, 0.5 - 0.25j, tb)
+    assert relerr(ta.cpu().numpy(), a + (0.5 - 0.25j) * b) < 1e-15
+    rb.scale(tb, 2j)
+    assert relerr(tb.cpu().numpy(), 2j * b) < 1e-15
+    f = torch.empty(1 << 14, dtype=torch.complex64, device=cuda)
+    rb.copy(f, tb)
+    assert relerr(f.cpu().numpy().astype(np.complex128), 2j * b) < 1e-7
+    r = rb.random_state(12, "c128", seed=5)
+    assert abs(rb.norm(r) - 1.0) < 1e-14
+    r2 = rb.random_state(12, "c128", seed=5)
+    assert torch.equal(r, r2)
