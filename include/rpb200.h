@@ -6,9 +6,10 @@
  * failure on the calling thread.  Vectors are device pointers to interleaved
  * complex numbers (RP_C64: float re/im, 8 bytes; RP_C128: double re/im, 16
  * bytes), 16-byte aligned, of length 2^len.  All calls are ordered on the
- * library's stream (rp_stream()); calls that return a scalar or copy to the
- * host synchronise it, matching the synchronous semantics of the reference's
- * GPUImpl (inc/gpuimpl.h:628-638).
+ * library's stream (rp_stream()), a blocking stream and therefore ordered
+ * with the legacy default stream both ways; calls that return a scalar or
+ * copy to the host synchronise it, matching the synchronous semantics of the
+ * reference's GPUImpl (inc/gpuimpl.h:628-638).
  *
  * Each entry point names the reference interface it replaces (paths inside
  * cl91/REAPERS).

@@ -458,11 +458,11 @@ static void launch_tiled(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream
     size_t smem = STAGES * TILE_BYTES + 2 * STAGES * sizeof(uint64_t) +
                   (DOTS ? (size_t)NW * l.ndot * 4 * sizeof(double) : 0);
     auto kern = k_apply_tiled<Real, B, P, STAGES, DOTS>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static size_t attr_smem = 0;
+    if (smem > attr_smem) {
         RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024));
-        attr_set = true;
+                                     (int)smem));
+        attr_smem = smem;
     }
     ApplyArgs<Real> a;
     a.in = static_cast<const Cplx<Real> *>(l.in);

@@ -15,15 +15,17 @@ namespace rp {
 //   jsign : bit j = parity(z_j & (j ^ xl_j)), the j-dependent part of the sign,
 //           z_j / xl_j being the bits of z / xl in the j field [log2 P, B)
 //   kind  : 0 real coefficient, 1 imaginary coefficient, 2 general complex
+// Records are 16-byte aligned (the kernel reads the four words as one uint4).
 template <typename Real>
-struct TermDesc {
+struct alignas(16) TermDesc {
     uint32_t xl, z, jsign, kind;
     Real cr, ci;
 };
+static_assert(sizeof(TermDesc<float>) == 32 && sizeof(TermDesc<double>) == 32, "layout");
 
 // A group of terms sharing the same high X-mask part xh = x >> B: they all
 // read the source tile (tile ^ xh).
-struct GroupDesc {
+struct alignas(16) GroupDesc {
     uint32_t xh, first, count, pad;
 };
 

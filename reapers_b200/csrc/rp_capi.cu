@@ -32,7 +32,10 @@ static void ensure_init() {
     if (e != cudaSuccess || n == 0) throw Error{RP_E_NODEVICE, "no CUDA device available"};
     if (g_device < 0) g_device = 0;
     RP_CUDA(cudaSetDevice(g_device));
-    RP_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+    // A blocking stream: work on it is ordered with the legacy default stream
+    // in both directions, so buffers written by a caller on the default stream
+    // (and reads of our results there) need no extra synchronisation.
+    RP_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamDefault));
 }
 
 static size_t esize(int dtype) { return dtype == RP_C128 ? 16 : 8; }
