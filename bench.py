@@ -1,0 +1,374 @@
+#!/usr/bin/env python3
+"""Benchmark of the REAPERS hot path on B200: Pauli-sum H.psi throughput.
+
+Workload (default, ``--config c4``): sparse SYK with N = 56 Majoranas on
+28 qubits (state of 2^28 complex64 = 2 GiB), k = 8, i.e. 448 quartic terms,
+H.psi in FP32.  ``--config c2``: sparse SYK N = 48 (24 qubits), 384 terms, FP64.
+
+A step is one H.psi product over the whole state.  The metric is H.psi HBM
+GB/s: the algorithmic bytes of one apply, (G + 1) * 2^L * sizeof(element)
+with G the number of distinct source tiles per output tile (every distinct
+tile read once per output tile, plus the write), divided by the device time
+of the kernel.  Inputs are larger than L2 (2 GiB vs 126 MB), so no flush is
+needed between steps.
+
+Multi-GPU (torchrun): every rank runs an independent replica (its own
+disorder realisation); no collective on the data path ("replicas only");
+the value is the sum over ranks of bytes / the max over ranks of time.
+
+``--impl reference`` times the reference's own CPU implementation
+(oracle/_ref/ref_driver: SpinOp::apply in CPUImpl::apply_ops's loop, OpenMP
+over all host threads) on a bounded slice of output rows of the same
+workload, in the same unit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("H·psi HBM GB/s; N=56 SYK OTOC pts/s, mixed+batched vs FP64 on B200 @1e-6")
+
+CONFIGS = {
+    "c4": dict(N=56, k=8, dtype="c64", workload="sparse SYK N=56 (28 qubits, 2^28 complex64 = 2 GiB), "
+               "k=8, 448 quartic terms, H.psi in FP32"),
+    "c2": dict(N=48, k=8, dtype="c128", workload="sparse SYK N=48 (24 qubits, 2^24 complex128 = 256 MiB), "
+               "k=8, 384 quartic terms, H.psi in FP64"),
+}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+PROFILE_SUMMARY = {"c4": "k_apply_tiled_sparse_syk_n56_fp32.md"}
+
+
+def profile_traffic(cfg_name):
+    """DRAM bytes (read + write) per launch of the apply kernel, from the
+    committed ncu summary of the same kernel and workload (None if absent)."""
+    name = PROFILE_SUMMARY.get(cfg_name)
+    p = os.path.join(ROOT, "profiles", name) if name else None
+    if p and os.path.exists(p):
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clk_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.index)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx = float(parts[1])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def make_terms(cfg, seed):
+    import reapers_b200 as rb
+    return rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed)
+
+
+def cpu_reference(cfg, bits, coeff, alg_bytes, rows, reps):
+    """Time the reference CPU apply on a slice of `rows` output rows."""
+    from oracle import oracle as O
+    L = cfg["N"] // 2
+    tmp = tempfile.mkdtemp(prefix="rpbench_")
+    tf = os.path.join(tmp, "terms")
+    O.write_terms(tf, L, bits, coeff)
+    fp = "32" if cfg["dtype"] == "c64" else "64"
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    env.setdefault("OMP_PROC_BIND", "close")
+    r = subprocess.run([O.REF_DRIVER, "bench_rows", tf, fp, "0", str(rows), str(reps)],
+                       capture_output=True, text=True, check=True, env=env)
+    d = json.loads(r.stdout)
+    D = 1 << L
+    return {"value": alg_bytes * (rows / D) / d["seconds"] / 1e9, "seconds": d["seconds"],
+            "threads": d["threads"], "rows": rows}
+
+
+def dist_setup(n):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def run_ours(args):
+    import torch
+    import reapers_b200 as rb
+
+    cfg = CONFIGS[args.config]
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    rb.init(local)
+    L = cfg["N"] // 2
+    bits, coeff = make_terms(cfg, seed=1000 + rank)
+    ham = rb.Hamiltonian(L, bits, coeff, cfg["dtype"])
+    info = ham.info()
+    alg = info["alg_bytes"]
+    x = rb.random_state(L, cfg["dtype"], seed=7 + rank, normalize=True)
+    y = torch.empty_like(x)
+    st = rb.stream()
+
+    if args.profile:
+        # one apply after a warm-up, for an ncu capture of the kernel
+        ham.apply(y, x)
+        rb.synchronize()
+        ham.apply(y, x)
+        rb.synchronize()
+        print(json.dumps({"profile": True, "info": info}))
+        return
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ham.apply(y, x)
+    torch.cuda.synchronize()
+    rb.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        ham.apply(y, x)
+    e1.record(st)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    t_step = e0.elapsed_time(e1) / 1e3 / args.steps
+    t_max = t_step
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = alg * world / t_max / 1e9
+    achieved = alg / t_step / 1e9
+
+    # end to end through the C ABI with host buffers: H2D of the state, apply,
+    # D2H of the result, every step
+    esize = 8 if cfg["dtype"] == "c64" else 16
+    nbytes = (1 << L) * esize
+    hx = torch.empty(1 << L, dtype=x.dtype, pin_memory=True)
+    hy = torch.empty_like(hx, pin_memory=True)
+    hx.copy_(x.cpu())
+    from reapers_b200 import _lib
+    import ctypes as C
+
+    def e2e_step():
+        _lib.call("rp_memcpy", C.c_void_p(x.data_ptr()), C.c_void_p(hx.data_ptr()), nbytes, 0)
+        ham.apply(y, x)
+        _lib.call("rp_memcpy", C.c_void_p(hy.data_ptr()), C.c_void_p(y.data_ptr()), nbytes, 1)
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    k2 = max(3, args.steps // 2)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(st)
+    for _ in range(k2):
+        e2e_step()
+    f1.record(st)
+    f1.synchronize()
+    t_e2e = f0.elapsed_time(f1) / 1e3 / k2
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e_value = alg * world / t_e2e / 1e9
+
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic(args.config)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_max * 1e3, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (complex64)" if cfg["dtype"] == "c64" else "f64 (complex128)",
+        "data": "synthetic: sparse SYK quartets drawn uniformly without replacement (seeded), "
+                "couplings N(0,1) x the reference's SYK scale; i.i.d. complex Gaussian state",
+        "config": {"workload": cfg["workload"], "tile_exp": info["tile_exp"],
+                   "source_tile_groups": info["ngroups"], "terms": info["nterms"],
+                   "alg_bytes_per_apply": alg, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state >> 126 MB), no flush"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes, "ms_per_step": round(t_e2e * 1e3, 3)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "term_applications_per_s": info["nterms"] * (1 << L) / t_step},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
+        try:
+            cb = cpu_reference(cfg, bits, coeff, alg, rows, 1)
+            line["cpu_baseline"] = {"value": round(cb["value"], 4), "unit": "GB/s",
+                                    "cores": cb["threads"], "kind": "reference",
+                                    "sample": f"reference SpinOp::apply over {rows} of 2^{L} "
+                                              f"output rows, same terms, OpenMP "
+                                              f"{cb['threads']} threads, {cb['seconds']:.2f} s"}
+        except Exception as e:   # the baseline is reported, never the target
+            line["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_driver was not built"}))
+        return
+    L = cfg["N"] // 2
+    bits, coeff = make_terms(cfg, seed=1000)
+    # the algorithmic bytes are those of our arm's plan (host-side grouping),
+    # so both arms report the same unit for the same work
+    alg = alg_bytes_host(L, bits, cfg["dtype"])
+    rows = 1 << 19 if cfg["N"] >= 56 else 1 << 17
+    times = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_reference(cfg, bits, coeff, alg, rows, 1)
+        if i >= args.warmup:
+            times.append(cb["seconds"])
+    t = float(np.mean(times))
+    value = alg * (rows / (1 << L)) / t / 1e9
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "impl": "reference",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (complex64)" if cfg["dtype"] == "c64" else "f64 (complex128)",
+            "data": "synthetic (same generator and seed as our arm)",
+            "config": {"workload": cfg["workload"],
+                       "sample": f"{rows} of 2^{L} output rows per step"},
+            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s",
+                             "cores": cb["threads"], "kind": "reference",
+                             "sample": f"{rows} of 2^{L} output rows per step"},
+            "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def alg_bytes_host(L, bits, dtype, tile_exp=12):
+    """(G + 1) * 2^L * element size for the default plan (G = distinct x >> B)."""
+    import reapers_b200.syk as S
+    B = min(tile_exp, max(5, L - 8))
+    x = S.xmask(bits)
+    G = len(np.unique(x >> np.uint64(B)))
+    return (G + 1) * (1 << L) * (8 if dtype == "c64" else 16)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c4")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--profile", action="store_true",
+                    help="run two applies and exit (for an ncu capture)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

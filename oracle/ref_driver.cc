@@ -1,6 +1,7 @@
 // ref_driver.cc -- runs the REAPERS reference library itself (its headers,
-// compiled unmodified from the reference checkout with REAPERS_NOGPU and
-// REAPERS_FP64, against the project-written Eigen subset in eigen_shim/).
+// compiled unmodified from the reference checkout with REAPERS_NOGPU and the
+// default (float) precision, as examples/syk.cc is, against the project-written
+// Eigen subset in eigen_shim/).
 //
 // TEST INFRASTRUCTURE ONLY: it makes golden fixtures, pins the C restatement
 // in rp_oracle.c, and is the timed CPU baseline (the reference's own
@@ -20,8 +21,10 @@
 #include <string>
 #include <vector>
 
+#include <omp.h>
+
 #define REAPERS_NOGPU
-#define REAPERS_FP64
+
 #include <reapers.h>
 
 using namespace REAPERS;
@@ -55,6 +58,10 @@ using Ops = HostSumOps<double>;
 using St = State<double, CountingImpl>;
 
 struct Term { uint64_t bits; double re, im; };
+
+static double now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 static std::vector<Term> read_terms(const char *path, int &len) {
     std::ifstream f(path, std::ios::binary);
@@ -94,13 +101,14 @@ static void write_terms(const char *path, const Ops &ops, int len) {
 // Build a SpinOp with the given internal bits and stored coefficient through
 // the public API: right-multiply single-site sigma matrices (no carry-over
 // sign arises between different sites), then fix the coefficient.
-static SpinOp<double> make_op(const Term &t) {
-    auto op = SpinOp<double>::identity();
+template <typename Fp>
+static SpinOp<Fp> make_op(const Term &t) {
+    auto op = SpinOp<Fp>::identity();
     for (int i = 0; i < 32; i++) {
         unsigned s = (t.bits >> (2 * i)) & 3;
-        if (s == 1) op *= SpinOp<double>::sigma_x(i);
-        else if (s == 2) op *= SpinOp<double>::sigma_z(i);
-        else if (s == 3) op *= SpinOp<double>::sigma_y(i);
+        if (s == 1) op *= SpinOp<Fp>::sigma_x(i);
+        else if (s == 2) op *= SpinOp<Fp>::sigma_z(i);
+        else if (s == 3) op *= SpinOp<Fp>::sigma_y(i);
     }
     // the coefficient is now i^ny; multiply by target * conj(i^ny) (exact)
     int ny = 0;
@@ -108,14 +116,50 @@ static SpinOp<double> make_op(const Term &t) {
     std::complex<double> cur(1, 0);
     for (int k = 0; k < (ny & 3); k++) cur *= std::complex<double>(0, 1);
     std::complex<double> f = std::complex<double>(t.re, t.im) * std::conj(cur);
-    op *= complex<double>(f.real(), f.imag());
+    op *= complex<Fp>((Fp)f.real(), (Fp)f.imag());
     return op;
 }
 
-static Ops build_ops(const std::vector<Term> &terms) {
-    Ops ops;
-    for (auto &t : terms) ops += make_op(t);
+template <typename Fp = double>
+static HostSumOps<Fp> build_ops(const std::vector<Term> &terms) {
+    HostSumOps<Fp> ops;
+    for (auto &t : terms) ops += make_op<Fp>(t);
     return ops;
+}
+
+// Time the body of CPUImpl::apply_ops (inc/cpuimpl.h:747-753) -- the
+// reference's SpinOp::apply per (row, term), terms in list order -- over the
+// bounded slice of output rows [row0, row0 + nrows) of a 2^len state, with
+// OpenMP over rows as the reference does.  Prints seconds per slice.
+template <typename Fp>
+static int bench_rows(const std::vector<Term> &terms, int len, uint64_t row0, uint64_t nrows,
+                      int reps) {
+    auto ops = build_ops<Fp>(terms);
+    const uint64_t D = 1ull << len;
+    std::vector<complex<Fp>> vec(D), res(nrows);
+    std::mt19937_64 g(12345);
+    std::normal_distribution<double> nd;
+    for (auto &v : vec) v = complex<Fp>((Fp)nd(g), (Fp)nd(g));
+    double best = 1e300;
+    for (int r = 0; r < reps; r++) {
+        double t0 = now();
+        #pragma omp parallel for schedule(static)
+        for (uint64_t i = 0; i < nrows; i++) {
+            complex<Fp> acc = 0;
+            for (const auto &op : ops) {
+                typename SpinOp<Fp>::StateType n = 0;
+                auto coeff = op.apply((typename SpinOp<Fp>::StateType)(row0 + i), n);
+                acc += coeff * vec[n];
+            }
+            res[i] = acc;
+        }
+        best = std::min(best, now() - t0);
+    }
+    double chk = 0;
+    for (auto &v : res) chk += std::abs(v);
+    printf("{\"seconds\": %.6e, \"rows\": %llu, \"len\": %d, \"terms\": %zu, \"threads\": %d, \"check\": %.6e}\n",
+           best, (unsigned long long)nrows, len, ops.size(), omp_get_max_threads(), chk);
+    return 0;
 }
 
 static std::vector<std::complex<double>> read_vec(const char *path) {
@@ -144,9 +188,6 @@ static std::vector<std::complex<double>> dump_state(const St &s) {
     return v;
 }
 
-static double now() {
-    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
 
 int main(int argc, char **argv) {
     if (argc < 2) { std::cerr << "usage: ref_driver MODE ...\n"; return 1; }
@@ -258,6 +299,16 @@ int main(int argc, char **argv) {
         double dt = (now() - t0) / reps;
         printf("{\"seconds_per_apply\": %.6e, \"len\": %d, \"terms\": %zu}\n", dt, len, ops.size());
         return 0;
+    }
+    if (mode == "bench_rows") {
+        // bench_rows terms fp(32|64) row0 nrows reps
+        int len; auto terms = read_terms(argv[2], len);
+        int fp = atoi(argv[3]);
+        uint64_t row0 = strtoull(argv[4], 0, 10), nrows = strtoull(argv[5], 0, 10);
+        int reps = atoi(argv[6]);
+        if (row0 + nrows > (1ull << len)) { std::cerr << "row slice out of range\n"; return 1; }
+        return fp == 32 ? bench_rows<float>(terms, len, row0, nrows, reps)
+                        : bench_rows<double>(terms, len, row0, nrows, reps);
     }
     std::cerr << "unknown mode " << mode << "\n";
     return 1;
