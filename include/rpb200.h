@@ -48,6 +48,11 @@ typedef struct {
     int stages;          /* shared-memory pipeline depth */
     int grid;            /* persistent CTAs */
     double alg_bytes;    /* (ngroups + 1) * 2^len * element size per apply */
+    int kernel;          /* 0 direct, 1 tiled (bulk copies), 2 rows (TMA, swizzled) */
+    int window;          /* CTAs in flight = aligned block of output tiles */
+    double alg_bytes_dram; /* (G_w + 1) * 2^len * element size, G_w = distinct
+                              x >> (tile_exp + log2 window): the compulsory DRAM
+                              bytes when source blocks are served from L2 */
 } rp_ham_info_t;
 
 /* Statistics of one evolve. */
@@ -109,7 +114,8 @@ int rp_vec_random(int dtype, uint64_t n, void *v, uint64_t seed);
  * inc/cpuimpl.h:233-253).  The table is grouped for the kernel here. */
 int rp_ham_create(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
                   const double *coeff);
-/* Same with an explicit tile exponent (5..12; 0 = default), for tuning. */
+/* Same with an explicit tile exponent (5..12) for the tiled kernel, for
+ * tuning and testing; 0 = default (the row kernel where it applies). */
 int rp_ham_create_ex(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uint64_t *bits,
                      const double *coeff, int tile_exp);
 int rp_ham_destroy(rp_ham_t h);

@@ -157,6 +157,9 @@ void plan_build(ApplyPlan &plan, int len, int dtype, const uint64_t *bits,
     else build_terms<float>(plan, bits, coeff, nterms);
     plan.ngroups = (int)plan.groups.size();
     plan.alg_bytes = (double)(plan.ngroups + 1) * D * (double)elem_size(dtype);
+    plan.rows = RowPlan{};
+    if (cfg.allow_rows) rowplan_build(plan.rows, len, dtype, bits, coeff, nterms);
+    if (plan.rows.ok) plan.alg_bytes = plan.rows.alg_bytes_smem;
 }
 
 void plan_upload(ApplyPlan &plan) {
@@ -173,6 +176,7 @@ void plan_upload(ApplyPlan &plan) {
     size_t gb = plan.groups.size() * sizeof(GroupDesc);
     RP_CUDA(cudaMalloc((void **)&plan.d_groups, gb ? gb : 16));
     if (gb) RP_CUDA(cudaMemcpy(plan.d_groups, plan.groups.data(), gb, cudaMemcpyHostToDevice));
+    if (plan.rows.ok) rowplan_upload(plan.rows);
 }
 
 void plan_free(ApplyPlan &plan) {
@@ -182,10 +186,12 @@ void plan_free(ApplyPlan &plan) {
     plan.d_terms = nullptr;
     plan.d_groups = nullptr;
     plan.d_direct = nullptr;
+    rowplan_free(plan.rows);
 }
 
 int apply_grid(const ApplyPlan &plan) {
     if (plan.cfg.direct) return 1;
+    if (plan.rows.ok) return plan.rows.window;
     return std::min(plan.ntiles, num_sms());
 }
 
@@ -532,6 +538,21 @@ void apply_launch(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream_t st) 
             const size_t pb = (size_t)apply_grid(plan) * l.ndot * 2 * sizeof(double);
             RP_CUDA(cudaMemsetAsync(l.partials, 0, pb, st));
         }
+        return;
+    }
+    if (plan.rows.ok) {
+        RowLaunch r;
+        r.in = l.in;
+        r.out = l.out;
+        r.alpha = l.alpha;
+        r.alpha_dev = l.alpha_dev;
+        r.accumulate = l.accumulate;
+        r.active = l.active;
+        r.dot_vecs = l.dot_vecs;
+        r.ndot = l.ndot;
+        r.partials = l.partials;
+        r.err = l.err;
+        rows_launch(plan.rows, plan.len, plan.dtype, r, st);
         return;
     }
     if (plan.dtype == 2) {

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "rp_apply_rows.cuh"
 #include "rp_common.cuh"
 
 namespace rp {
@@ -37,6 +38,7 @@ struct ApplyConfig {
     int P = 0;        // consumer threads per CTA
     int stages = 0;   // shared-memory pipeline depth
     bool direct = false;   // tiny vectors: one thread per element, no tiling
+    bool allow_rows = true;   // use the row-layout kernel when it applies
 };
 
 // Host copy of a grouped term table plus its device image.
@@ -55,6 +57,7 @@ struct ApplyPlan {
     void *d_direct = nullptr;
     double alg_bytes = 0;   // (ngroups + 1) * D * sizeof(element): one read of
                             // every distinct source tile per output tile + the write
+    RowPlan rows;           // row-layout kernel (used when rows.ok)
 };
 
 // Build the grouped table for the given configuration (host only; no GPU).

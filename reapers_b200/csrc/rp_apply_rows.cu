@@ -1,0 +1,478 @@
+// Row-layout H.psi kernel for sm_100a (the default for large states).
+//
+// Each source tile (256 rows x 128 bytes = 32 KB: 4096 complex64 or 2048
+// complex128 elements) is brought into shared memory by one 2-D TMA tensor
+// copy with the 128-byte swizzle, so the 16-byte chunk p of row r lands at
+// chunk p ^ (r & 7).  Consumer thread t owns output row t: per term it reads
+// the whole source row t ^ xr (eight conflict-free 16-byte loads), applies
+// the in-row permutation u -> u ^ xc as a compile-time register permutation
+// (a warp-uniform switch over the 2C cases xc + C*kind), the column sign from
+// a per-term bit mask, and accumulates into registers.  Output rows are
+// written once.  Complex coefficients are split into a real and an imaginary
+// term on the host, so every term costs two FMAs per element.
+//
+// Tile order: the grid is a power of two (128 CTAs when there are enough
+// tiles) and CTA c handles tiles c, c + grid, ...: the output tiles in flight
+// form an aligned block of `grid` tiles, whose source tiles for a group xh are
+// the aligned block (block ^ (xh >> log2 grid)).  Groups are visited in
+// increasing xh, so groups sharing xh >> log2 grid read the same source block
+// back to back and it is served from L2: DRAM bytes per apply are
+// (G_w + 1) D s with G_w = distinct x >> (B + log2 grid).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "rp_apply.cuh"
+#include "rp_apply_rows.cuh"
+
+namespace rp {
+
+static int log2i(uint64_t v) {
+    int l = 0;
+    while ((1ull << l) < v) l++;
+    return l;
+}
+
+void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
+                   int64_t nterms) {
+    rp = RowPlan{};
+    const int esz = dtype == 2 ? 16 : 8;
+    const int C = 128 / esz;
+    const int logC = log2i(C);
+    const int B = logC + 8;
+    if (len < B + 7) return;   // fewer than 128 tiles: the first-generation kernel
+    struct T {
+        uint32_t x, z;
+        double c;
+        int kind;
+    };
+    std::vector<T> ts;
+    for (int64_t k = 0; k < nterms; k++) {
+        uint32_t x = 0, z = 0;
+        for (int i = 0; i < len; i++) {
+            x |= (uint32_t)((bits[k] >> (2 * i)) & 1) << i;
+            z |= (uint32_t)((bits[k] >> (2 * i + 1)) & 1) << i;
+        }
+        const double cr = coeff[2 * k], ci = coeff[2 * k + 1];
+        if (cr != 0.0 || ci == 0.0) ts.push_back({x, z, cr, 0});
+        if (ci != 0.0) ts.push_back({x, z, ci, 1});
+    }
+    if ((int)ts.size() > ROW_MAX_TERMS) return;
+    std::stable_sort(ts.begin(), ts.end(),
+                     [B](const T &a, const T &b) { return (a.x >> B) < (b.x >> B); });
+    for (size_t k = 0; k < ts.size(); k++) {
+        const uint32_t xh = ts[k].x >> B;
+        if (rp.groups.empty() || rp.groups.back().xh != xh)
+            rp.groups.push_back({xh, (uint32_t)k, 0u, 0u});
+        rp.groups.back().count++;
+        const uint32_t xl = ts[k].x & ((1u << B) - 1);
+        const uint32_t xr = xl >> logC, xc = xl & (uint32_t)(C - 1);
+        const uint32_t zc = ts[k].z & (uint32_t)(C - 1);
+        uint32_t js = 0;
+        for (int u = 0; u < C; u++) js |= (uint32_t)(__builtin_popcount(zc & (u ^ xc)) & 1) << u;
+        RowTerm<float> r{};
+        r.cs = xr | ((xc + (uint32_t)C * ts[k].kind) << 16);
+        r.z = ts[k].z;
+        r.js = js;
+        r.cf = (float)ts[k].c;
+        r.cd = ts[k].c;
+        rp.terms.push_back(r);
+    }
+    if ((int)rp.groups.size() > ROW_MAX_GROUPS) {
+        rp = RowPlan{};
+        return;
+    }
+    rp.ok = true;
+    rp.B = B;
+    rp.logC = logC;
+    rp.ntiles = 1 << (len - B);
+    rp.nterms = (int)rp.terms.size();
+    rp.window = std::min(rp.ntiles, 128);
+    const double D = std::ldexp(1.0, len);
+    std::vector<uint32_t> hw;
+    for (auto &g : rp.groups) hw.push_back(g.xh >> log2i(rp.window));
+    hw.erase(std::unique(hw.begin(), hw.end()), hw.end());
+    rp.alg_bytes_smem = (double)(rp.groups.size() + 1) * D * esz;
+    rp.alg_bytes_dram = (double)(hw.size() + 1) * D * esz;
+}
+
+void rowplan_upload(RowPlan &rp) {
+    if (!rp.ok) return;
+    rowplan_free(rp);
+    RP_CUDA(cudaMalloc(&rp.d_terms, std::max<size_t>(16, rp.terms.size() * sizeof(RowTerm<float>))));
+    RP_CUDA(cudaMemcpy(rp.d_terms, rp.terms.data(), rp.terms.size() * sizeof(RowTerm<float>),
+                       cudaMemcpyHostToDevice));
+    RP_CUDA(cudaMalloc((void **)&rp.d_groups, std::max<size_t>(16, rp.groups.size() * sizeof(RowGroup))));
+    RP_CUDA(cudaMemcpy(rp.d_groups, rp.groups.data(), rp.groups.size() * sizeof(RowGroup),
+                       cudaMemcpyHostToDevice));
+}
+
+void rowplan_free(RowPlan &rp) {
+    if (rp.d_terms) cudaFree(rp.d_terms);
+    if (rp.d_groups) cudaFree(rp.d_groups);
+    rp.d_terms = nullptr;
+    rp.d_groups = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Device code
+// ---------------------------------------------------------------------------
+template <typename Real>
+__device__ __forceinline__ Real sgn_flip(Real c, uint32_t sb);
+template <>
+__device__ __forceinline__ float sgn_flip<float>(float c, uint32_t sb) {
+    return __uint_as_float(__float_as_uint(c) ^ sb);
+}
+template <>
+__device__ __forceinline__ double sgn_flip<double>(double c, uint32_t sb) {
+    return __longlong_as_double(__double_as_longlong(c) ^ ((long long)sb << 32));
+}
+
+template <typename Real>
+struct RowArgs {
+    Cplx<Real> *out;
+    const RowTerm<float> *terms;
+    const RowGroup *groups;
+    int nterms, ngroups, ntiles, stages;
+    double alpha;
+    const double *alpha_dev;
+    int accumulate;
+    const int *active;
+    const Cplx<Real> *const *dot_vecs;
+    int ndot;
+    double *partials;
+    unsigned *err;
+};
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// acc[u] += c_u * v[u ^ XC] (KIND 0) or i c_u * v[u ^ XC] (KIND 1),
+// c_u = c0 with the sign bit flipped where bit u of js is set.
+template <typename Real, int C, int K>
+__device__ __forceinline__ void row_case(Cplx<Real> (&acc)[C], const Cplx<Real> (&v)[C], Real c0,
+                                         uint32_t js) {
+    if constexpr (K < 2 * C) {
+        constexpr int XC = K % C, KIND = K / C;
+#pragma unroll
+        for (int u = 0; u < C; u++) {
+            const uint32_t sb = (js << (31 - u)) & 0x80000000u;
+            const Real c = sgn_flip(c0, sb);
+            const Cplx<Real> s = v[u ^ XC];
+            if (KIND == 0) {
+                acc[u].x = fma(c, s.x, acc[u].x);
+                acc[u].y = fma(c, s.y, acc[u].y);
+            } else {
+                acc[u].x = fma(-c, s.y, acc[u].x);
+                acc[u].y = fma(c, s.x, acc[u].y);
+            }
+        }
+    }
+}
+
+#define RP_RC(K) \
+    case K: row_case<Real, C, K>(acc, v, c0, js); break;
+
+template <typename Real, int C>
+__device__ __forceinline__ void row_dispatch(int cas, Cplx<Real> (&acc)[C], const Cplx<Real> (&v)[C],
+                                             Real c0, uint32_t js) {
+    switch (cas) {
+        RP_RC(0) RP_RC(1) RP_RC(2) RP_RC(3) RP_RC(4) RP_RC(5) RP_RC(6) RP_RC(7)
+        RP_RC(8) RP_RC(9) RP_RC(10) RP_RC(11) RP_RC(12) RP_RC(13) RP_RC(14) RP_RC(15)
+        RP_RC(16) RP_RC(17) RP_RC(18) RP_RC(19) RP_RC(20) RP_RC(21) RP_RC(22) RP_RC(23)
+        RP_RC(24) RP_RC(25) RP_RC(26) RP_RC(27) RP_RC(28) RP_RC(29) RP_RC(30) RP_RC(31)
+        default: break;
+    }
+}
+#undef RP_RC
+
+constexpr int ROW_P = 256;          // consumer threads = rows per tile
+constexpr int ROW_NW = ROW_P / 32;
+constexpr unsigned ROW_TILE_BYTES = 256 * 128;
+
+template <typename Real>
+__global__ void __launch_bounds__(ROW_P + 32, 1)
+    k_apply_rows(const __grid_constant__ CUtensorMap tmap, const RowArgs<Real> a) {
+    constexpr int C = 128 / (int)sizeof(Cplx<Real>);
+    constexpr int LOGC = C == 16 ? 4 : 3;
+    constexpr int B = LOGC + 8;
+    extern __shared__ unsigned char smem_raw[];
+    // 1024-byte alignment for the 128-byte swizzle pattern
+    unsigned char *smem = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int S = a.stages;
+    unsigned char *stage = smem;
+    RowTerm<float> *sterms = reinterpret_cast<RowTerm<float> *>(smem + (size_t)S * ROW_TILE_BYTES);
+    RowGroup *sgroups = reinterpret_cast<RowGroup *>(sterms + a.nterms);
+    uint64_t *full = reinterpret_cast<uint64_t *>(sgroups + a.ngroups);
+    uint64_t *empty = full + S;
+    double *red = reinterpret_cast<double *>(empty + S);
+    __shared__ int s_abort;
+    __shared__ long s_issued;
+
+    if (a.active && *a.active == 0) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < a.nterms; i += blockDim.x) sterms[i] = a.terms[i];
+    for (int i = tid; i < a.ngroups; i += blockDim.x) sgroups[i] = a.groups[i];
+    if (a.ndot)
+        for (int i = tid; i < ROW_NW * a.ndot * 4; i += blockDim.x) red[i] = 0.0;
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], ROW_NW);
+        }
+        s_abort = 0;
+        s_issued = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    const int ntile_iters =
+        (int)blockIdx.x < a.ntiles ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const long total = (long)ntile_iters * a.ngroups;
+
+    if (warp == ROW_NW) {
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap))
+                         : "memory");
+            long it = 0;
+            for (; it < total; ++it) {
+                const int s = (int)(it % S);
+                const unsigned round = (unsigned)(it / S);
+                if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, a.err)) {
+                    atomicExch(&s_abort, 1);
+                    break;
+                }
+                const long ti = it / a.ngroups;
+                const int g = (int)(it - ti * a.ngroups);
+                const uint32_t o = blockIdx.x + (uint32_t)ti * gridDim.x;
+                const uint32_t src = o ^ sgroups[g].xh;
+                mbar_arrive_expect_tx(&full[s], ROW_TILE_BYTES);
+                tma_load_2d(stage + (size_t)s * ROW_TILE_BYTES, &tmap, 0, (int)(src * 256u), &full[s]);
+            }
+            s_issued = it;
+        }
+    } else {
+        const uint32_t t = (uint32_t)tid;
+        const double scale = a.alpha * (a.alpha_dev ? *a.alpha_dev : 1.0);
+        long it = 0;
+        bool ok = true;
+        for (int ti = 0; ti < ntile_iters && ok; ++ti) {
+            const uint32_t o = blockIdx.x + (uint32_t)ti * gridDim.x;
+            Cplx<Real> acc[C];
+#pragma unroll
+            for (int u = 0; u < C; u++) acc[u].x = acc[u].y = Real(0);
+            for (int g = 0; g < a.ngroups; ++g, ++it) {
+                const int s = (int)(it % S);
+                const unsigned round = (unsigned)(it / S);
+                const RowGroup gd = sgroups[g];
+                const uint32_t src_hi = (o ^ gd.xh) << B;
+                if (!mbar_wait_bounded(&full[s], round & 1u, a.err)) {
+                    ok = false;
+                    break;
+                }
+                const unsigned char *tile = stage + (size_t)s * ROW_TILE_BYTES;
+                for (uint32_t k = gd.first; k < gd.first + gd.count; ++k) {
+                    const RowTerm<float> &tk = sterms[k];
+                    const uint32_t cs = tk.cs, z = tk.z, js = tk.js;
+                    const uint32_t sr = t ^ (cs & 0xFFFFu);
+                    const uint32_t m0 = src_hi | (sr << LOGC);
+                    const uint32_t s0 = (uint32_t)(__popc(z & m0) & 1) << 31;
+                    Real c0;
+                    if constexpr (sizeof(Real) == 4) c0 = sgn_flip(tk.cf, s0);
+                    else c0 = sgn_flip(tk.cd, s0);
+                    // the source row, un-swizzling 16-byte chunks
+                    const unsigned char *row = tile + sr * 128u;
+                    const uint32_t swz = (sr & 7u) << 4;
+                    Cplx<Real> v[C];
+#pragma unroll
+                    for (int p = 0; p < 8; p++) {
+                        const float4 q =
+                            *reinterpret_cast<const float4 *>(row + (((uint32_t)p << 4) ^ swz));
+                        if constexpr (sizeof(Real) == 4) {
+                            v[2 * p].x = q.x;
+                            v[2 * p].y = q.y;
+                            v[2 * p + 1].x = q.z;
+                            v[2 * p + 1].y = q.w;
+                        } else {
+                            const double2 d = *reinterpret_cast<const double2 *>(&q);
+                            v[p].x = d.x;
+                            v[p].y = d.y;
+                        }
+                    }
+                    row_dispatch<Real, C>((int)(cs >> 16), acc, v, c0, js);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[s]);
+            }
+            if (!ok) break;
+            // write the row: C contiguous elements = 8 x 16 bytes
+            Cplx<Real> *orow = a.out + ((size_t)o << B) + (size_t)t * C;
+#pragma unroll
+            for (int u = 0; u < C; u++) {
+                Cplx<Real> r;
+                r.x = (Real)(scale * (double)acc[u].x);
+                r.y = (Real)(scale * (double)acc[u].y);
+                acc[u] = r;
+            }
+            if (a.accumulate) {
+#pragma unroll
+                for (int u = 0; u < C; u++) {
+                    const Cplx<Real> old = orow[u];
+                    acc[u].x += old.x;
+                    acc[u].y += old.y;
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < 8; p++) {
+                float4 q;
+                if constexpr (sizeof(Real) == 4) {
+                    q = make_float4(acc[2 * p].x, acc[2 * p].y, acc[2 * p + 1].x, acc[2 * p + 1].y);
+                } else {
+                    const double2 d = make_double2(acc[p].x, acc[p].y);
+                    q = *reinterpret_cast<const float4 *>(&d);
+                }
+                reinterpret_cast<float4 *>(orow)[p] = q;
+            }
+            if (a.ndot) {
+                for (int i = 0; i < a.ndot; i++) {
+                    const Cplx<Real> *u = a.dot_vecs[i] + ((size_t)o << B) + (size_t)t * C;
+                    double sr = 0.0, si = 0.0;
+#pragma unroll
+                    for (int e = 0; e < C; e++) {
+                        const Cplx<Real> uv = u[e];
+                        sr = fma((double)uv.x, (double)acc[e].x, fma((double)uv.y, (double)acc[e].y, sr));
+                        si = fma((double)uv.x, (double)acc[e].y, fma(-(double)uv.y, (double)acc[e].x, si));
+                    }
+                    sr = warp_sum(sr);
+                    si = warp_sum(si);
+                    if (lane == 0) {
+                        double *r = red + ((size_t)warp * a.ndot + i) * 4;
+                        double s, e;
+                        two_sum(r[0], sr, s, e);
+                        r[0] = s;
+                        r[1] += e;
+                        two_sum(r[2], si, s, e);
+                        r[2] = s;
+                        r[3] += e;
+                    }
+                }
+            }
+        }
+        if (!ok) atomicExch(&s_abort, 1);
+    }
+    __syncthreads();
+    if (s_abort) {
+        if (tid == 0) {
+            const long issued = s_issued;
+            for (long it = issued - S; it < issued; ++it) {
+                if (it < 0) continue;
+                mbar_wait_bounded(&full[it % S], (unsigned)((it / S) & 1), a.err);
+            }
+        }
+        return;
+    }
+    if (a.ndot) {
+        for (int i = tid; i < a.ndot; i += blockDim.x) {
+            CompSum re, im;
+            for (int w = 0; w < ROW_NW; w++) {
+                const double *r = red + ((size_t)w * a.ndot + i) * 4;
+                re.add(r[0]);
+                re.add(r[1]);
+                im.add(r[2]);
+                im.add(r[3]);
+            }
+            a.partials[((size_t)blockIdx.x * a.ndot + i) * 2 + 0] = re.value();
+            a.partials[((size_t)blockIdx.x * a.ndot + i) * 2 + 1] = im.value();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host launch
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        RP_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        RP_REQUIRE(q == cudaDriverEntryPointSuccess && p, -3, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// The state viewed as rows of 128 bytes: inner dimension 32 floats (or 16
+// doubles), outer dimension D / C rows; box = one 256-row tile, 128B swizzle.
+static CUtensorMap make_row_map(const void *base, int len, int dtype) {
+    CUtensorMap m;
+    const int esz = dtype == 2 ? 16 : 8;
+    const int C = 128 / esz;
+    const cuuint64_t inner = dtype == 2 ? 16 : 32;
+    const cuuint64_t dims[2] = {inner, (cuuint64_t)((1ull << len) / C)};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {(cuuint32_t)inner, 256};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = get_encode()(
+        &m, dtype == 2 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+        const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    RP_REQUIRE(r == CUDA_SUCCESS, -3, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+template <typename Real>
+static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch &l,
+                          cudaStream_t st) {
+    const size_t fixed = (size_t)rp.nterms * sizeof(RowTerm<float>) +
+                         (size_t)rp.groups.size() * sizeof(RowGroup) +
+                         (size_t)ROW_NW * l.ndot * 4 * sizeof(double) + 1024;
+    const size_t budget = 227 * 1024 - 64;   // opt-in limit minus static shared memory
+    int S = (int)std::min<size_t>(6, (budget - fixed - 16 * 8) / (ROW_TILE_BYTES + 16));
+    RP_REQUIRE(S >= 2, -2, "Hamiltonian table too large for the row kernel");
+    const size_t smem = (size_t)S * ROW_TILE_BYTES + fixed + (size_t)2 * S * sizeof(uint64_t);
+    auto kern = k_apply_rows<Real>;
+    static size_t attr = 0;
+    if (smem > attr) {
+        RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = smem;
+    }
+    RowArgs<Real> a;
+    a.out = static_cast<Cplx<Real> *>(l.out);
+    a.terms = static_cast<const RowTerm<float> *>(rp.d_terms);
+    a.groups = rp.d_groups;
+    a.nterms = rp.nterms;
+    a.ngroups = (int)rp.groups.size();
+    a.ntiles = rp.ntiles;
+    a.stages = S;
+    a.alpha = l.alpha;
+    a.alpha_dev = l.alpha_dev;
+    a.accumulate = l.accumulate;
+    a.active = l.active;
+    a.dot_vecs = reinterpret_cast<const Cplx<Real> *const *>(l.dot_vecs);
+    a.ndot = l.ndot;
+    a.partials = l.partials;
+    a.err = l.err;
+    const CUtensorMap map = make_row_map(l.in, len, dtype);
+    kern<<<rp.window, ROW_P + 32, smem, st>>>(map, a);
+    RP_CUDA(cudaGetLastError());
+}
+
+void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st) {
+    RP_REQUIRE(rp.ok, -2, "row kernel not planned for this Hamiltonian");
+    RP_REQUIRE(l.ndot <= 64, -2, "too many fused projections");
+    if (dtype == 2) launch_rows_t<double>(rp, len, dtype, l, st);
+    else launch_rows_t<float>(rp, len, dtype, l, st);
+}
+
+}  // namespace rp

@@ -1,0 +1,69 @@
+// Row-layout H.psi kernel (second generation): host-side table and launch.
+#pragma once
+
+#include <vector>
+
+#include "rp_common.cuh"
+
+namespace rp {
+
+// A source/output tile is 256 rows of 128 bytes (16 complex64 or 8
+// complex128 elements per row); consumer thread t owns output row t.
+// For a term with in-tile X part xl: source row = t ^ xr (xr = xl >> logC),
+// source column for output column u = u ^ xc (xc = xl & (C-1)).
+// cs packs xr (bits 0-15) and the kernel's code case xc + C*kind (bits 16-23).
+// js: bit u = parity(zc & (u ^ xc)) with zc = z & (C-1), the column-dependent
+// part of the sign.  kind 0: real coefficient c, kind 1: imaginary (i c).
+template <typename Real>
+struct alignas(16) RowTerm {
+    uint32_t cs, z, js;
+    float cf;      // coefficient, FP32 kernels
+    double cd;     // coefficient, FP64 kernels
+    double pad;
+};
+static_assert(sizeof(RowTerm<float>) == 32, "layout");
+
+struct alignas(16) RowGroup {
+    uint32_t xh, first, count, pad;
+};
+
+struct RowPlan {
+    bool ok = false;          // the row kernel applies to this Hamiltonian
+    int B = 0, logC = 0;      // tile exponent, log2(elements per row)
+    int ntiles = 0;
+    int nterms = 0;           // after splitting complex coefficients
+    std::vector<RowTerm<float>> terms;
+    std::vector<RowGroup> groups;
+    void *d_terms = nullptr;
+    RowGroup *d_groups = nullptr;
+    int window = 0;           // CTAs of an aligned tile window (grid size)
+    double alg_bytes_smem = 0;  // (G + 1) D s, G = distinct x >> B
+    double alg_bytes_dram = 0;  // (G_w + 1) D s, G_w = distinct x >> (B + log2 window)
+};
+
+// Largest Hamiltonian (terms after splitting, groups) the row kernel stages
+// in shared memory.
+constexpr int ROW_MAX_TERMS = 2048;
+constexpr int ROW_MAX_GROUPS = 1024;
+
+void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
+                   int64_t nterms);
+void rowplan_upload(RowPlan &rp);
+void rowplan_free(RowPlan &rp);
+
+struct RowLaunch {
+    const void *in = nullptr;
+    void *out = nullptr;
+    double alpha = 1.0;
+    const double *alpha_dev = nullptr;
+    int accumulate = 0;
+    const int *active = nullptr;
+    const void *const *dot_vecs = nullptr;
+    int ndot = 0;
+    double *partials = nullptr;   // [grid][ndot][2]
+    unsigned *err = nullptr;
+};
+
+void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st);
+
+}  // namespace rp

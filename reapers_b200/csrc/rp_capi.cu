@@ -257,6 +257,7 @@ int rp_ham_create_ex(rp_ham_t *h, int len, int dtype, uint64_t nterms, const uin
             RP_REQUIRE(tile_exp >= 5 && tile_exp <= 12 && tile_exp <= len, RP_E_INVALID,
                        "tile_exp must be in [5, min(12, len)]");
             cfg.direct = false;
+            cfg.allow_rows = false;
             cfg.B = tile_exp;
             cfg.P = std::min(256, 1 << tile_exp);
         }
@@ -300,6 +301,15 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info) {
         info->stages = p.cfg.direct ? 0 : p.cfg.stages;
         info->grid = apply_grid(p);
         info->alg_bytes = p.alg_bytes;
+        info->kernel = p.cfg.direct ? 0 : (p.rows.ok ? 2 : 1);
+        info->window = apply_grid(p);
+        info->alg_bytes_dram = p.rows.ok ? p.rows.alg_bytes_dram : p.alg_bytes;
+        if (p.rows.ok) {
+            info->tile_exp = p.rows.B;
+            info->ngroups = (int)p.rows.groups.size();
+            info->threads = 256;
+            info->nterms = p.rows.nterms;
+        }
     });
 }
 

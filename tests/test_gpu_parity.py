@@ -183,3 +183,44 @@ def test_vector_ops(cuda):
     assert abs(rb.norm(r) - 1.0) < 1e-14
     r2 = rb.random_state(12, "c128", seed=5)
     assert torch.equal(r, r2)
+
+
+@pytest.mark.parametrize("L,dtype", [(18, "c128"), (19, "c64"), (20, "c128"), (20, "c64")])
+def test_apply_row_kernel(cuda, L, dtype):
+    """The TMA row-layout kernel (default for >= 18/19 qubits), including
+    complex coefficients (split into a real and an imaginary term) and a
+    fused projection through the Krylov path."""
+    N = 2 * L
+    bits, coeff = rb.syk.sparse_syk(N, k=4, seed=L)
+    rng = np.random.default_rng(L)
+    # a few general terms with complex coefficients and low X/Z bits
+    extra = rng.integers(0, 1 << (2 * L), size=12, dtype=np.uint64)
+    bits = np.concatenate([bits, extra])
+    coeff = np.concatenate([coeff, 0.01 * (rng.standard_normal(12) + 1j * rng.standard_normal(12))])
+    bits, idx = np.unique(bits, return_index=True)
+    coeff = coeff[idx]
+    v = rand_vec(rng, L)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    assert ham.info()["kernel"] == 2
+    x = to_dev(v, dtype)
+    out = torch.empty_like(x)
+    ham.apply(out, x)
+    ref = O.apply(L, bits, coeff, v)
+    tol = FP64_TOL if dtype == "c128" else FP32_TOL
+    assert relerr(out.cpu().numpy().astype(np.complex128), ref) < tol
+    ham.apply(out, x, accumulate=True)
+    assert relerr(out.cpu().numpy().astype(np.complex128), 2 * ref) < tol
+
+
+def test_evolve_row_kernel_fp64(cuda):
+    L, N = 18, 36
+    bits, coeff = rb.syk.sparse_syk(N, k=8, seed=4)
+    v = rand_vec(np.random.default_rng(2), L)
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    assert ham.info()["kernel"] == 2
+    x = to_dev(v, "c128")
+    st = rb.evolve(ham, x, 0.8, 0.0, 6, 1e-10)
+    ref, st2 = O.evolve(L, bits, coeff, v, 0.8, 0.0, 6, 1e-10)
+    assert relerr(x.cpu().numpy(), ref) < FP64_TOL
+    for key in ("restarts", "applies", "passes", "prods"):
+        assert st[key] == st2[key], (key, st, st2)
