@@ -2,26 +2,29 @@
 //
 // Each source tile (256 rows x 128 bytes = 32 KB: 4096 complex64 or 2048
 // complex128 elements) is brought into shared memory by one 2-D TMA tensor
-// copy with the 128-byte swizzle, so the 16-byte chunk p of row r lands at
-// chunk p ^ (r & 7).  Consumer thread t owns output row t: per term it reads
-// the whole source row t ^ xr (eight conflict-free 16-byte loads), applies
-// the in-row permutation u -> u ^ xc as a compile-time register permutation
-// (a warp-uniform switch over the 2C cases xc + C*kind), the column sign from
-// a per-term bit mask, and accumulates into registers.  Output rows are
+// copy with the 128-byte swizzle: the 16-byte chunk q of row r lands at chunk
+// q ^ (r & 7).  Consumer thread t owns output row t.  For a term with in-tile
+// X part xl = (xr, xq, x0) -- row XOR, chunk XOR, element-in-chunk XOR -- the
+// source of output element (t, chunk p, e) is (t ^ xr, chunk p ^ xq, e ^ x0).
+// The chunk XOR folds into the swizzle XOR of the shared-memory address, so
+// the in-row permutation costs nothing; only the swap inside a 16-byte chunk
+// (x0, FP32 only), its sign (z0) and the coefficient kind remain, as eight
+// compile-time cases chosen by a warp-uniform switch.  The column-dependent
+// sign is one select per chunk from a per-term 8-bit mask.  Output rows are
 // written once.  Complex coefficients are split into a real and an imaginary
 // term on the host, so every term costs two FMAs per element.
 //
-// Tile order: the grid is a power of two (128 CTAs when there are enough
-// tiles) and CTA c handles tiles c, c + grid, ...: the output tiles in flight
-// form an aligned block of `grid` tiles, whose source tiles for a group xh are
-// the aligned block (block ^ (xh >> log2 grid)).  Groups are visited in
-// increasing xh, so groups sharing xh >> log2 grid read the same source block
-// back to back and it is served from L2: DRAM bytes per apply are
-// (G_w + 1) D s with G_w = distinct x >> (B + log2 grid).
+// Tile order: CTA c handles tiles c, c + grid, ...; the output tiles in
+// flight form a block of `grid` consecutive tiles, whose source tiles for a
+// group xh are that block XOR xh.  Groups are visited in increasing xh, so
+// groups sharing the high bits of xh read overlapping source blocks back to
+// back from L2.  Two CTAs per SM (2 x 148 = 296 CTAs) give 16 consumer warps
+// per SM to hide shared-memory and FMA latency.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "rp_apply.cuh"
@@ -39,8 +42,10 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
                    int64_t nterms) {
     rp = RowPlan{};
     const int esz = dtype == 2 ? 16 : 8;
-    const int C = 128 / esz;
+    const int C = 128 / esz;         // elements per row
+    const int EPC = 16 / esz;        // elements per 16-byte chunk
     const int logC = log2i(C);
+    const int logE = log2i(EPC);
     const int B = logC + 8;
     if (len < B + 7) return;   // fewer than 128 tiles: the first-generation kernel
     struct T {
@@ -69,13 +74,16 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
         rp.groups.back().count++;
         const uint32_t xl = ts[k].x & ((1u << B) - 1);
         const uint32_t xr = xl >> logC, xc = xl & (uint32_t)(C - 1);
+        const uint32_t xq = xc >> logE, x0 = xc & (uint32_t)(EPC - 1);
         const uint32_t zc = ts[k].z & (uint32_t)(C - 1);
-        uint32_t js = 0;
-        for (int u = 0; u < C; u++) js |= (uint32_t)(__builtin_popcount(zc & (u ^ xc)) & 1) << u;
+        const uint32_t zq = zc >> logE, z0 = zc & (uint32_t)(EPC - 1);
+        // chunk sign: bit p = parity(zq & (p ^ xq)) (source chunk p ^ xq)
+        uint32_t jc = 0;
+        for (int p = 0; p < 8; p++) jc |= (uint32_t)(__builtin_popcount(zq & (p ^ xq)) & 1) << p;
         RowTerm<float> r{};
-        r.cs = xr | ((xc + (uint32_t)C * ts[k].kind) << 16);
+        r.cs = xr | (xq << 8) | ((x0 | (z0 << 1) | ((uint32_t)ts[k].kind << 2)) << 11);
         r.z = ts[k].z;
-        r.js = js;
+        r.js = jc;
         r.cf = (float)ts[k].c;
         r.cd = ts[k].c;
         rp.terms.push_back(r);
@@ -89,10 +97,17 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
     rp.logC = logC;
     rp.ntiles = 1 << (len - B);
     rp.nterms = (int)rp.terms.size();
-    rp.window = std::min(rp.ntiles, 128);
+    // CTAs in flight: two per SM by default (measured fastest on B200:
+    // 47.7 ms vs 67.3 ms with one per SM and 77.6 ms with an aligned
+    // 128-CTA window at N = 56); RPB200_ROW_GRID overrides it for tuning.
+    int win = 2 * num_sms();
+    if (const char *e = getenv("RPB200_ROW_GRID")) win = std::max(1, atoi(e));
+    rp.window = std::min(rp.ntiles, win);
     const double D = std::ldexp(1.0, len);
     std::vector<uint32_t> hw;
-    for (auto &g : rp.groups) hw.push_back(g.xh >> log2i(rp.window));
+    int lw = 0;
+    while ((2 << lw) <= rp.window) lw++;
+    for (auto &g : rp.groups) hw.push_back(g.xh >> lw);
     hw.erase(std::unique(hw.begin(), hw.end()), hw.end());
     rp.alg_bytes_smem = (double)(rp.groups.size() + 1) * D * esz;
     rp.alg_bytes_dram = (double)(hw.size() + 1) * D * esz;
@@ -120,17 +135,6 @@ void rowplan_free(RowPlan &rp) {
 // Device code
 // ---------------------------------------------------------------------------
 template <typename Real>
-__device__ __forceinline__ Real sgn_flip(Real c, uint32_t sb);
-template <>
-__device__ __forceinline__ float sgn_flip<float>(float c, uint32_t sb) {
-    return __uint_as_float(__float_as_uint(c) ^ sb);
-}
-template <>
-__device__ __forceinline__ double sgn_flip<double>(double c, uint32_t sb) {
-    return __longlong_as_double(__double_as_longlong(c) ^ ((long long)sb << 32));
-}
-
-template <typename Real>
 struct RowArgs {
     Cplx<Real> *out;
     const RowTerm<float> *terms;
@@ -155,53 +159,62 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// acc[u] += c_u * v[u ^ XC] (KIND 0) or i c_u * v[u ^ XC] (KIND 1),
-// c_u = c0 with the sign bit flipped where bit u of js is set.
-template <typename Real, int C, int K>
-__device__ __forceinline__ void row_case(Cplx<Real> (&acc)[C], const Cplx<Real> (&v)[C], Real c0,
-                                         uint32_t js) {
-    if constexpr (K < 2 * C) {
-        constexpr int XC = K % C, KIND = K / C;
+// One term over a whole row.  w[p], loaded from rq ^ (p << 4), holds source
+// chunk p ^ xq (the permutation is in the address); case K = x0 | z0 << 1 | kind << 2.  Output
+// element u = EPC p + e takes source element e ^ x0 of w[p] with sign
+// (chunk sign p) * (-1)^(z0 & (e ^ x0)).
+template <typename Real, int K>
+__device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
+                                           uint32_t rq, Real c0, uint32_t jc) {
+    constexpr int EPC = 16 / (int)sizeof(Cplx<Real>);
+    constexpr int X0 = K & 1, Z0 = (K >> 1) & 1, KIND = K >> 2;
+    if constexpr (EPC == 1 && (X0 || Z0)) {
+        return;
+    } else {
+        const Real cn = -c0;
+        float4 w[8];
 #pragma unroll
-        for (int u = 0; u < C; u++) {
-            const uint32_t sb = (js << (31 - u)) & 0x80000000u;
-            const Real c = sgn_flip(c0, sb);
-            const Cplx<Real> s = v[u ^ XC];
-            if (KIND == 0) {
-                acc[u].x = fma(c, s.x, acc[u].x);
-                acc[u].y = fma(c, s.y, acc[u].y);
-            } else {
-                acc[u].x = fma(-c, s.y, acc[u].x);
-                acc[u].y = fma(c, s.x, acc[u].y);
+        for (int p = 0; p < 8; p++) {
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(w[p].x), "=f"(w[p].y), "=f"(w[p].z), "=f"(w[p].w)
+                         : "r"(rq ^ ((uint32_t)p << 4)));
+        }
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            const Real cp = ((jc >> p) & 1u) ? cn : c0;
+#pragma unroll
+            for (int e = 0; e < EPC; e++) {
+                const int se = e ^ X0;
+                Real vx, vy;
+                if constexpr (EPC == 2) {
+                    vx = se ? w[p].z : w[p].x;
+                    vy = se ? w[p].w : w[p].y;
+                } else {
+                    vx = __hiloint2double(__float_as_int(w[p].y), __float_as_int(w[p].x));
+                    vy = __hiloint2double(__float_as_int(w[p].w), __float_as_int(w[p].z));
+                }
+                const Real c = (Z0 & se) ? -cp : cp;
+                Cplx<Real> &a = acc[EPC * p + e];
+                if (KIND == 0) {
+                    a.x = fma(c, vx, a.x);
+                    a.y = fma(c, vy, a.y);
+                } else {
+                    a.x = fma(-c, vy, a.x);
+                    a.y = fma(c, vx, a.y);
+                }
             }
         }
     }
 }
 
-#define RP_RC(K) \
-    case K: row_case<Real, C, K>(acc, v, c0, js); break;
-
-template <typename Real, int C>
-__device__ __forceinline__ void row_dispatch(int cas, Cplx<Real> (&acc)[C], const Cplx<Real> (&v)[C],
-                                             Real c0, uint32_t js) {
-    switch (cas) {
-        RP_RC(0) RP_RC(1) RP_RC(2) RP_RC(3) RP_RC(4) RP_RC(5) RP_RC(6) RP_RC(7)
-        RP_RC(8) RP_RC(9) RP_RC(10) RP_RC(11) RP_RC(12) RP_RC(13) RP_RC(14) RP_RC(15)
-        RP_RC(16) RP_RC(17) RP_RC(18) RP_RC(19) RP_RC(20) RP_RC(21) RP_RC(22) RP_RC(23)
-        RP_RC(24) RP_RC(25) RP_RC(26) RP_RC(27) RP_RC(28) RP_RC(29) RP_RC(30) RP_RC(31)
-        default: break;
-    }
-}
-#undef RP_RC
-
 constexpr int ROW_P = 256;          // consumer threads = rows per tile
 constexpr int ROW_NW = ROW_P / 32;
 constexpr unsigned ROW_TILE_BYTES = 256 * 128;
 
-template <typename Real>
-__global__ void __launch_bounds__(ROW_P + 32, 1)
+template <typename Real, int MINB>
+__global__ void __launch_bounds__(ROW_P + 32, MINB)
     k_apply_rows(const __grid_constant__ CUtensorMap tmap, const RowArgs<Real> a) {
-    constexpr int C = 128 / (int)sizeof(Cplx<Real>);
+    constexpr int C = 128 / (int)sizeof(Cplx<Real>);   // elements per row
     constexpr int LOGC = C == 16 ? 4 : 3;
     constexpr int B = LOGC + 8;
     extern __shared__ unsigned char smem_raw[];
@@ -261,7 +274,7 @@ __global__ void __launch_bounds__(ROW_P + 32, 1)
             s_issued = it;
         }
     } else {
-        const uint32_t t = (uint32_t)tid;
+        const uint32_t row = (uint32_t)tid;
         const double scale = a.alpha * (a.alpha_dev ? *a.alpha_dev : 1.0);
         long it = 0;
         bool ok = true;
@@ -279,43 +292,37 @@ __global__ void __launch_bounds__(ROW_P + 32, 1)
                     ok = false;
                     break;
                 }
-                const unsigned char *tile = stage + (size_t)s * ROW_TILE_BYTES;
+                const uint32_t tile = smem_u32(stage + (size_t)s * ROW_TILE_BYTES);
                 for (uint32_t k = gd.first; k < gd.first + gd.count; ++k) {
-                    const RowTerm<float> &tk = sterms[k];
-                    const uint32_t cs = tk.cs, z = tk.z, js = tk.js;
-                    const uint32_t sr = t ^ (cs & 0xFFFFu);
-                    const uint32_t m0 = src_hi | (sr << LOGC);
-                    const uint32_t s0 = (uint32_t)(__popc(z & m0) & 1) << 31;
+                    const uint4 d0 = *reinterpret_cast<const uint4 *>(&sterms[k]);
+                    const uint32_t cs = d0.x, z = d0.y, jc = d0.z;
+                    const uint32_t sr = row ^ (cs & 0xFFu);
+                    const uint32_t xq = (cs >> 8) & 7u;
+                    const uint32_t s0 = (uint32_t)(__popc(z & (src_hi | (sr << LOGC))) & 1);
                     Real c0;
-                    if constexpr (sizeof(Real) == 4) c0 = sgn_flip(tk.cf, s0);
-                    else c0 = sgn_flip(tk.cd, s0);
-                    // the source row, un-swizzling 16-byte chunks
-                    const unsigned char *row = tile + sr * 128u;
-                    const uint32_t swz = (sr & 7u) << 4;
-                    Cplx<Real> v[C];
-#pragma unroll
-                    for (int p = 0; p < 8; p++) {
-                        const float4 q =
-                            *reinterpret_cast<const float4 *>(row + (((uint32_t)p << 4) ^ swz));
-                        if constexpr (sizeof(Real) == 4) {
-                            v[2 * p].x = q.x;
-                            v[2 * p].y = q.y;
-                            v[2 * p + 1].x = q.z;
-                            v[2 * p + 1].y = q.w;
-                        } else {
-                            const double2 d = *reinterpret_cast<const double2 *>(&q);
-                            v[p].x = d.x;
-                            v[p].y = d.y;
-                        }
+                    if constexpr (sizeof(Real) == 4) c0 = __uint_as_float(d0.w);
+                    else c0 = sterms[k].cd;
+                    if (s0) c0 = -c0;
+                    // chunk p of the permuted source row sits at physical
+                    // chunk p ^ xq ^ (sr & 7) of row sr
+                    const uint32_t rq = (tile + sr * 128u) | ((xq ^ (sr & 7u)) << 4);
+                    switch ((cs >> 11) & 7u) {
+                        case 0: chunk_case<Real, 0>(acc, rq, c0, jc); break;
+                        case 1: chunk_case<Real, 1>(acc, rq, c0, jc); break;
+                        case 2: chunk_case<Real, 2>(acc, rq, c0, jc); break;
+                        case 3: chunk_case<Real, 3>(acc, rq, c0, jc); break;
+                        case 4: chunk_case<Real, 4>(acc, rq, c0, jc); break;
+                        case 5: chunk_case<Real, 5>(acc, rq, c0, jc); break;
+                        case 6: chunk_case<Real, 6>(acc, rq, c0, jc); break;
+                        default: chunk_case<Real, 7>(acc, rq, c0, jc); break;
                     }
-                    row_dispatch<Real, C>((int)(cs >> 16), acc, v, c0, js);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[s]);
             }
             if (!ok) break;
             // write the row: C contiguous elements = 8 x 16 bytes
-            Cplx<Real> *orow = a.out + ((size_t)o << B) + (size_t)t * C;
+            Cplx<Real> *orow = a.out + ((size_t)o << B) + (size_t)row * C;
 #pragma unroll
             for (int u = 0; u < C; u++) {
                 Cplx<Real> r;
@@ -337,14 +344,16 @@ __global__ void __launch_bounds__(ROW_P + 32, 1)
                 if constexpr (sizeof(Real) == 4) {
                     q = make_float4(acc[2 * p].x, acc[2 * p].y, acc[2 * p + 1].x, acc[2 * p + 1].y);
                 } else {
-                    const double2 d = make_double2(acc[p].x, acc[p].y);
-                    q = *reinterpret_cast<const float4 *>(&d);
+                    q = make_float4(__int_as_float(__double2loint(acc[p].x)),
+                                    __int_as_float(__double2hiint(acc[p].x)),
+                                    __int_as_float(__double2loint(acc[p].y)),
+                                    __int_as_float(__double2hiint(acc[p].y)));
                 }
                 reinterpret_cast<float4 *>(orow)[p] = q;
             }
             if (a.ndot) {
                 for (int i = 0; i < a.ndot; i++) {
-                    const Cplx<Real> *u = a.dot_vecs[i] + ((size_t)o << B) + (size_t)t * C;
+                    const Cplx<Real> *u = a.dot_vecs[i] + ((size_t)o << B) + (size_t)row * C;
                     double sr = 0.0, si = 0.0;
 #pragma unroll
                     for (int e = 0; e < C; e++) {
@@ -437,15 +446,22 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     const size_t fixed = (size_t)rp.nterms * sizeof(RowTerm<float>) +
                          (size_t)rp.groups.size() * sizeof(RowGroup) +
                          (size_t)ROW_NW * l.ndot * 4 * sizeof(double) + 1024;
-    const size_t budget = 227 * 1024 - 64;   // opt-in limit minus static shared memory
+    // CTAs per SM (RPB200_ROW_CTAS, 1 or 2; default 2): the shared memory of
+    // an SM (228 KB, 1 KB of it reserved per CTA) is split between them
+    static int ctas = 0;
+    if (!ctas) {
+        const char *e = getenv("RPB200_ROW_CTAS");
+        ctas = (e && atoi(e) == 1) ? 1 : 2;
+    }
+    const size_t budget = (ctas == 2 ? 113 * 1024 : 227 * 1024) - 64;
     int S = (int)std::min<size_t>(6, (budget - fixed - 16 * 8) / (ROW_TILE_BYTES + 16));
     RP_REQUIRE(S >= 2, -2, "Hamiltonian table too large for the row kernel");
     const size_t smem = (size_t)S * ROW_TILE_BYTES + fixed + (size_t)2 * S * sizeof(uint64_t);
-    auto kern = k_apply_rows<Real>;
-    static size_t attr = 0;
-    if (smem > attr) {
+    auto kern = ctas == 2 ? k_apply_rows<Real, 2> : k_apply_rows<Real, 1>;
+    static size_t attr[2] = {0, 0};
+    if (smem > attr[ctas - 1]) {
         RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
+        attr[ctas - 1] = smem;
     }
     RowArgs<Real> a;
     a.out = static_cast<Cplx<Real> *>(l.out);

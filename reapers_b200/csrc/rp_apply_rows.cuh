@@ -7,13 +7,14 @@
 
 namespace rp {
 
-// A source/output tile is 256 rows of 128 bytes (16 complex64 or 8
-// complex128 elements per row); consumer thread t owns output row t.
-// For a term with in-tile X part xl: source row = t ^ xr (xr = xl >> logC),
-// source column for output column u = u ^ xc (xc = xl & (C-1)).
-// cs packs xr (bits 0-15) and the kernel's code case xc + C*kind (bits 16-23).
-// js: bit u = parity(zc & (u ^ xc)) with zc = z & (C-1), the column-dependent
-// part of the sign.  kind 0: real coefficient c, kind 1: imaginary (i c).
+// A source/output tile is 256 rows of 128 bytes = 8 chunks of 16 bytes (16
+// complex64 or 8 complex128 elements per row); consumer thread t owns output
+// row t.  For a term with in-tile X part xl = (xr, xq, x0) -- row, chunk and
+// element-in-chunk XOR -- output element (t, p, e) reads (t ^ xr, p ^ xq,
+// e ^ x0).  cs packs xr (bits 0-7), xq (bits 8-10) and the code case
+// x0 | z0 << 1 | kind << 2 (bits 11-13), z0 being the element-in-chunk bit of
+// the Z mask.  js: bit p = parity(zq & (p ^ xq)), the chunk-dependent part of
+// the sign (zq = chunk bits of z).  kind 0: real coefficient, 1: imaginary.
 template <typename Real>
 struct alignas(16) RowTerm {
     uint32_t cs, z, js;
