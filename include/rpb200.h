@@ -100,6 +100,16 @@ int rp_vec_scale(int dtype, uint64_t n, void *v, double ar, double ai);
 /* GPUImpl::vec_prod: out[0] + i out[1] = <a|b> (conjugate-linear in a),
  * FP64 compensated accumulation */
 int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out);
+/* Same result as rp_vec_dot, but allocates no device memory: for callers
+ * that cannot let a library call cudaMalloc (a framework that owns all
+ * device memory through its own allocator, or a loop in which cudaMalloc /
+ * cudaFree would implicitly synchronise the device).  No counterpart in the
+ * reference.  Its scratch is a fixed 16 KB device array (1024 partial sums),
+ * so n may be at most 2^28 (larger n returns RP_E_INVALID with a message).
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race.  Runs on the legacy default stream. */
+int rp_vec_dot_noalloc(int dtype, uint64_t n, const void *a, const void *b, double *out);
 /* GPUImpl::vec_norm */
 int rp_vec_norm(int dtype, uint64_t n, const void *v, double *out);
 /* GPUImpl::init_random without the normalisation: i.i.d. complex Gaussian

@@ -56,6 +56,7 @@ _SIGS = {
     "rp_vec_add": (C.c_int, [C.c_int, C.c_uint64, _VP, _VP, _VP]),
     "rp_vec_scale": (C.c_int, [C.c_int, C.c_uint64, _VP, C.c_double, C.c_double]),
     "rp_vec_dot": (C.c_int, [C.c_int, C.c_uint64, _VP, _VP, C.POINTER(C.c_double)]),
+    "rp_vec_dot_noalloc": (C.c_int, [C.c_int, C.c_uint64, _VP, _VP, C.POINTER(C.c_double)]),
     "rp_vec_norm": (C.c_int, [C.c_int, C.c_uint64, _VP, C.POINTER(C.c_double)]),
     "rp_vec_random": (C.c_int, [C.c_int, C.c_uint64, _VP, C.c_uint64]),
     "rp_ham_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, C.c_uint64,
