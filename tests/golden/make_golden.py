@@ -1,0 +1,104 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in this directory by running the reference
+library itself (oracle/_ref/ref_driver: the REAPERS headers compiled as a CPU
+program).  Run in a checkout where the reference is present:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Fixtures (numpy .npz):
+  majorana_N{N}.npz        reference Majorana strings b_0..b_{N-1}, N = 4..20
+  syk_dense_N8_seed5.npz   SYK::gen_ham(std::mt19937(5)) term list, N = 8
+  c1_dense_syk_N24.npz     dense SYK N = 24 (12 qubits, 10626 terms) from
+                           SYK::gen_ham(std::mt19937(1)), psi0, and
+                           State::evolve results at t = 0.5, 2.5, 5.0 (m = 20,
+                           tol = 1e-12) with the reference's call counts
+  apply_L10.npz            random terms, vector and State operator* output
+  evolve_sparse_N20.npz    sparse SYK N = 20 (seeded project generator),
+                           evolve at (t, beta) = (1.5, 0.25), m = 8
+  otoc_N16.npz             dense SYK N = 16 from gen_ham(mt19937(3)),
+                           F(t) at t = 0, 0.5, 1, 2 in the order of
+                           examples/simple-syk-krylov.cc (m = 10, tol 1e-12)
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+import reapers_b200.syk as S  # noqa: E402
+
+
+def main():
+    R = O.RefDriver(threads=8)
+    for N in range(4, 22, 2):
+        L, b, c = R.majorana(N)
+        np.savez_compressed(os.path.join(HERE, f"majorana_N{N}.npz"), bits=b, coeff=c)
+    L, b, c = R.syk(8, 0.0, 1.0, 5)
+    np.savez_compressed(os.path.join(HERE, "syk_dense_N8_seed5.npz"), bits=b, coeff=c, len=L)
+
+    # C1: dense SYK N = 24, reference generator
+    L, b, c = R.syk(24, 0.0, 1.0, 1)
+    rng = np.random.default_rng(2024)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    times = [0.5, 2.5, 5.0]
+    outs, applies, prods = [], [], []
+    for t in times:
+        o, st = R.evolve(L, b, c, psi, t, 0.0, 20, 1e-12)
+        outs.append(o)
+        applies.append(st["applies"])
+        prods.append(st["prods"])
+    np.savez_compressed(os.path.join(HERE, "c1_dense_syk_N24.npz"), bits=b, coeff=c, len=L,
+                        psi0=psi, times=np.array(times), out=np.array(outs),
+                        applies=np.array(applies), prods=np.array(prods), krydim=20, tol=1e-12)
+
+    # apply: random terms with every coefficient kind
+    rng = np.random.default_rng(7)
+    L = 10
+    bits = np.unique(rng.integers(0, 1 << (2 * L), size=60, dtype=np.uint64))
+    coeff = rng.standard_normal(len(bits)) + 1j * rng.standard_normal(len(bits))
+    coeff[::3] = coeff[::3].real
+    coeff[1::3] = 1j * coeff[1::3].imag
+    v = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    rt_len, rt_bits, rt_coeff = R.roundtrip(L, bits, coeff)
+    out = R.apply(L, bits, coeff, v)
+    np.savez_compressed(os.path.join(HERE, "apply_L10.npz"), bits=bits, coeff=coeff, len=L,
+                        vec=v, out=out, rt_bits=rt_bits, rt_coeff=rt_coeff)
+
+    # evolve with imaginary time as well (sparse SYK from the project generator)
+    L = 10
+    bits, coeff = S.sparse_syk(20, k=4, seed=33)
+    rng = np.random.default_rng(8)
+    v = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    v /= np.linalg.norm(v)
+    o, st = R.evolve(L, bits, coeff, v, 1.5, 0.25, 8, 1e-12)
+    np.savez_compressed(os.path.join(HERE, "evolve_sparse_N20.npz"), bits=bits, coeff=coeff,
+                        len=L, psi0=v, t=1.5, beta=0.25, krydim=8, tol=1e-12, out=o,
+                        applies=st["applies"], prods=st["prods"])
+
+    # OTOC: the example's operator order, W = b_{N-1}, V = b_{N-2}
+    N = 16
+    L, b, c = R.syk(N, 0.0, 1.0, 3)
+    _, mb, mc = R.majorana(N)
+    w = (mb[N - 1:N], mc[N - 1:N])
+    vv = (mb[N - 2:N - 1], mc[N - 2:N - 1])
+    rng = np.random.default_rng(9)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    times = [0.0, 0.5, 1.0, 2.0]
+    vals, st = R.otoc(L, b, c, w, vv, psi, times, 10, 1e-12)
+    np.savez_compressed(os.path.join(HERE, "otoc_N16.npz"), bits=b, coeff=c, len=L,
+                        w_bits=w[0], w_coeff=w[1], v_bits=vv[0], v_coeff=vv[1], psi0=psi,
+                        times=np.array(times), F=vals, krydim=10, tol=1e-12,
+                        applies=st["applies"])
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

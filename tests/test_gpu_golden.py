@@ -1,0 +1,69 @@
+"""GPU results against golden fixtures made by the reference library itself
+(tests/golden/make_golden.py): FP64 within 1e-12 relative, operation counts
+exact."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import reapers_b200 as rb
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def dev(v):
+    return torch.from_numpy(np.ascontiguousarray(v)).cuda()
+
+
+def test_apply_reference_fixture(cuda):
+    g = gold("apply_L10.npz")
+    L = int(g["len"])
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    out = torch.empty(1 << L, dtype=torch.complex128, device=cuda)
+    ham.apply(out, dev(g["vec"]))
+    o = out.cpu().numpy()
+    assert np.linalg.norm(o - g["out"]) / np.linalg.norm(g["out"]) < 1e-13
+
+
+def test_c1_dense_syk_evolve_reference_fixture(cuda):
+    """C1: dense SYK N = 24 (12 qubits, all 10626 quartets from the
+    reference's SYK::gen_ham), m = 20, tol 1e-12, t = 0.5, 2.5, 5.0."""
+    g = gold("c1_dense_syk_N24.npz")
+    L = int(g["len"])
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    for k, t in enumerate(g["times"]):
+        x = dev(g["psi0"])
+        st = rb.evolve(ham, x, float(t), 0.0, int(g["krydim"]), float(g["tol"]))
+        o = x.cpu().numpy()
+        assert np.linalg.norm(o - g["out"][k]) / np.linalg.norm(g["out"][k]) < 1e-12
+        assert st["applies"] == g["applies"][k]
+        assert st["prods"] == g["prods"][k]
+
+
+def test_imaginary_time_evolve_reference_fixture(cuda):
+    g = gold("evolve_sparse_N20.npz")
+    L = int(g["len"])
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    x = dev(g["psi0"])
+    st = rb.evolve(ham, x, float(g["t"]), float(g["beta"]), int(g["krydim"]), float(g["tol"]))
+    o = x.cpu().numpy()
+    assert np.linalg.norm(o - g["out"]) / np.linalg.norm(g["out"]) < 1e-12
+    assert st["applies"] == int(g["applies"]) and st["prods"] == int(g["prods"])
+
+
+def test_otoc_reference_fixture(cuda):
+    g = gold("otoc_N16.npz")
+    L = int(g["len"])
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    w = rb.Hamiltonian(L, g["w_bits"], g["w_coeff"], "c128")
+    v = rb.Hamiltonian(L, g["v_bits"], g["v_coeff"], "c128")
+    vals, applies = rb.otoc(ham, w, v, dev(g["psi0"]), g["times"], int(g["krydim"]),
+                            float(g["tol"]))
+    assert np.abs(vals - g["F"]).max() < 1e-12
+    assert applies == int(g["applies"])
