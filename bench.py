@@ -141,6 +141,60 @@ def on_chip_bound(info, L, cfg, t_step, clocks):
             "frac": round(ach / peak, 4)}
 
 
+def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
+    """N = 56 OTOC F(t) = <psi0| W(t) V W(t) V |psi0> (W = b_{N-1}, V = b_{N-2},
+    the operators of examples/simple-syk-krylov.cc) on a bounded sample of the
+    C4 time grid (t = 0 and the first `npts` points of 20 on [0, 15]), one
+    disorder realisation x one state, m = 16, for the plain FP64 path
+    (reference default tol = FP64 epsilon) and the mixed path (FP32 vectors
+    and H.psi, FP64 inner products / Hessenberg / expm, tol = FP32 epsilon).
+    Error: max |F_mixed - F_fp64| / |F_fp64(0)| over the sampled points."""
+    import torch
+    import reapers_b200 as rb
+    L = cfg["N"] // 2
+    N = cfg["N"]
+    grid = np.linspace(0.0, 15.0, 20)
+    times = [0.0] + list(grid[1:1 + npts])
+    mb, mc = rb.syk.majoranas(N)
+    out = {"workload": f"sparse SYK N={N} (2^{L}), k={cfg['k']}, 1 realisation x 1 state, "
+                       f"t in {[float(round(t, 4)) for t in times]} of the 20-point grid on [0, 15], "
+                       f"m={krydim}",
+           "operators": "W = b_{N-1}, V = b_{N-2} (non-block Majoranas)"}
+    psi64 = rb.random_state(L, "c128", seed=seed, normalize=True)
+    res = {}
+    for name, dt, tol in (("fp64_plain", "c128", float(np.finfo(np.float64).eps)),
+                          ("mixed_fp32", "c64", float(np.finfo(np.float32).eps))):
+        ham = rb.Hamiltonian(L, bits, coeff, dt)
+        w = rb.Hamiltonian(L, mb[N - 1:N], mc[N - 1:N], dt)
+        v = rb.Hamiltonian(L, mb[N - 2:N - 1], mc[N - 2:N - 1], dt)
+        if dt == "c128":
+            psi0 = psi64
+        else:
+            psi0 = torch.empty(1 << L, dtype=torch.complex64, device="cuda")
+            rb.copy(psi0, psi64)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        vals, applies = rb.otoc(ham, w, v, psi0, times, krydim, tol)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        res[name] = vals
+        npt = len(times) - 1   # t = 0 costs no evolve
+        out[name] = {"seconds": round(el, 3), "pts_per_s": round(npt / el, 5),
+                     "applies": int(applies), "tol": tol,
+                     "F": [[round(z.real, 10), round(z.imag, 10)] for z in vals]}
+        del ham, w, v
+        if dt == "c64":
+            del psi0
+        rb._lib.call("rp_workspace_release")
+        torch.cuda.empty_cache()
+    f0 = abs(res["fp64_plain"][0])
+    err = float(np.max(np.abs(res["mixed_fp32"] - res["fp64_plain"])) / f0)
+    out["mixed_max_rel_err_vs_fp64"] = err
+    out["speedup_mixed_vs_fp64"] = round(out["fp64_plain"]["seconds"] /
+                                         out["mixed_fp32"]["seconds"], 3)
+    return out
+
+
 def make_terms(cfg, seed):
     import reapers_b200 as rb
     return rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed)
@@ -309,6 +363,10 @@ def run_ours(args):
                      "term_applications_per_s": info["nterms"] * (1 << L) / t_step},
         "clocks": clocks,
     }
+    if args.config == "c4" and not args.no_otoc:
+        del x, y, ham
+        torch.cuda.empty_cache()
+        line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
@@ -384,6 +442,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c4")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
+    ap.add_argument("--otoc-points", type=int, default=2,
+                    help="non-zero time points of the C4 grid in the OTOC sample")
     ap.add_argument("--profile", action="store_true",
                     help="run two applies and exit (for an ncu capture)")
     args = ap.parse_args()
