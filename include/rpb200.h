@@ -147,6 +147,30 @@ int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double t
 /* Free the cached Krylov workspace (krydim + 2 vectors). */
 int rp_workspace_release(void);
 
+/* --- batched OTOC (the outer loops of examples/syk.cc:417-475 and
+ * examples/simple-syk-krylov.cc:42-57 over many disorder realisations and
+ * states, run as one persistent launch per time step) ---------------------- */
+typedef struct rp_batch *rp_batch_t;
+/* nprob problems; problem p has len[p] qubits (8..30), nterms[p] terms
+ * (bits[p], coeff[p] as for rp_ham_create), W and V single Pauli strings
+ * (wbits[p], wcoeff[2p..2p+1]; vbits[p], vcoeff[...]), an initial complex64
+ * device state psi0[p] (kept, not modified), and a tile exponent tile[p]
+ * (8..11, 0 = default; tile may be NULL).  FP32 vectors, FP64 Krylov
+ * internals; krydim <= 32; every evolve stops after max_restarts restarts
+ * (1..64) or when ||Hexp0|| < tol. */
+int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nterms,
+                    const uint64_t *const *bits, const double *const *coeff,
+                    const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
+                    const double *vcoeff, const void *const *psi0, const int *tile, int krydim,
+                    double tol, int max_restarts);
+/* F[(p * ntimes + k) * 2 + {0,1}] = <psi0| W(t_k) V W(t_k) V |psi0> of problem
+ * p (beta = 0), applies[p * ntimes + k] its H.psi count (either may be NULL).
+ * One persistent launch per time step; with use_graph the launches are
+ * captured once into a CUDA graph and replayed. */
+int rp_batch_otoc(rp_batch_t b, int ntimes, const double *times, double *F, int *applies,
+                  int use_graph);
+int rp_batch_destroy(rp_batch_t b);
+
 #ifdef __cplusplus
 }
 #endif

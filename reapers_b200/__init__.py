@@ -177,6 +177,69 @@ def random_state(length, dtype="c128", seed=0, normalize=True, device="cuda"):
     return t
 
 
+class BatchOTOC:
+    """Many independent OTOC problems (disorder realisations x states, uneven
+    qubit counts) run by one persistent launch per time step (rp_batch_*).
+
+    problems: list of dicts with keys len, bits, coeff, w (bits, coeff),
+    v (bits, coeff), psi0 (complex64 CUDA tensor) and optionally tile (8..11).
+    FP32 vectors, FP64 Krylov internals (the mixed-precision form)."""
+
+    def __init__(self, problems, krydim=16, tol=1.2e-7, max_restarts=16):
+        n = len(problems)
+        self._keep = problems
+        lens = (C.c_int * n)(*[int(p["len"]) for p in problems])
+        self._bits = [np.ascontiguousarray(p["bits"], dtype=np.uint64) for p in problems]
+        self._coeff = [np.ascontiguousarray(p["coeff"], dtype=np.complex128).view(np.float64)
+                       for p in problems]
+        nterms = (C.c_int64 * n)(*[len(b) for b in self._bits])
+        bitp = (C.POINTER(C.c_uint64) * n)(*[b.ctypes.data_as(C.POINTER(C.c_uint64))
+                                             for b in self._bits])
+        coefp = (C.POINTER(C.c_double) * n)(*[c.ctypes.data_as(C.POINTER(C.c_double))
+                                              for c in self._coeff])
+        wb = (C.c_uint64 * n)(*[int(np.asarray(p["w"][0]).ravel()[0]) for p in problems])
+        vb = (C.c_uint64 * n)(*[int(np.asarray(p["v"][0]).ravel()[0]) for p in problems])
+        wc = (C.c_double * (2 * n))()
+        vc = (C.c_double * (2 * n))()
+        for i, p in enumerate(problems):
+            a = complex(np.asarray(p["w"][1]).ravel()[0])
+            b = complex(np.asarray(p["v"][1]).ravel()[0])
+            wc[2 * i], wc[2 * i + 1] = a.real, a.imag
+            vc[2 * i], vc[2 * i + 1] = b.real, b.imag
+        for p in problems:
+            if _tcode(p["psi0"]) != RP_C64:
+                raise ValueError("batched states are complex64")
+        psis = (C.c_void_p * n)(*[p["psi0"].data_ptr() for p in problems])
+        tiles = (C.c_int * n)(*[int(p.get("tile", 0)) for p in problems])
+        h = C.c_void_p()
+        _lib.call("rp_batch_create", C.byref(h), n, lens, nterms, bitp, coefp, wb, wc, vb, vc,
+                  psis, tiles, int(krydim), float(tol), int(max_restarts))
+        self._h = h
+        self.n = n
+
+    def run(self, times, use_graph=True):
+        """Returns (F[n, ntimes] complex, applies[n, ntimes])."""
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        k = len(times)
+        F = np.zeros(2 * self.n * k)
+        ap = np.zeros(self.n * k, np.int32)
+        _lib.call("rp_batch_otoc", self._h, k, times.ctypes.data_as(C.POINTER(C.c_double)),
+                  F.ctypes.data_as(C.POINTER(C.c_double)),
+                  ap.ctypes.data_as(C.POINTER(C.c_int)), 1 if use_graph else 0)
+        return F.view(np.complex128).reshape(self.n, k), ap.reshape(self.n, k)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().rp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def otoc(ham, w, v, psi0, times, krydim=5, tol=None):
     """F(t) = <psi0| W(t) V W(t) V |psi0> at beta = 0, in the operation order of
     examples/simple-syk-krylov.cc:42-57 (psi = V psi0; e^{-iHt}; W; e^{iHt};

@@ -69,6 +69,15 @@ _SIGS = {
     "rp_evolve": (C.c_int, [_VP, _VP, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                             C.POINTER(EvolveStats)]),
     "rp_workspace_release": (C.c_int, []),
+    "rp_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint64)),
+                                  C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_double), C.POINTER(_VP), C.POINTER(C.c_int),
+                                  C.c_int, C.c_double, C.c_int]),
+    "rp_batch_otoc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int), C.c_int]),
+    "rp_batch_destroy": (C.c_int, [_VP]),
 }
 
 

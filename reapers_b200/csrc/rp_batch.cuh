@@ -1,0 +1,55 @@
+// Batched OTOC: many independent (disorder realisation, random state)
+// problems, uneven qubit counts, one persistent launch per time step.
+#pragma once
+
+#include <vector>
+
+#include "rp_apply.cuh"
+
+namespace rp {
+
+// One problem as the persistent kernel reads it (FP32 state, FP64 Krylov).
+struct alignas(16) BatchProblem {
+    const TermDesc<float> *terms;   // grouped by x >> B (tiled-kernel records)
+    const GroupDesc *groups;
+    const Cplx<float> *psi0;        // initial state (device)
+    int len, B, ntiles, ngroups;
+    uint32_t wx, wz, vx, vz;        // W and V Pauli strings (X, Z masks)
+    float wcr, wci, vcr, vci;       // their coefficients
+};
+
+struct BatchPlan {
+    int nprob = 0, krydim = 0, max_restarts = 0, hcap = 0;
+    double tol = 0;
+    int maxB = 0, maxlen = 0, nslots = 0;
+    std::vector<ApplyPlan> plans;            // per problem (host tables + device copies)
+    std::vector<BatchProblem> probs;         // device-pointer records, largest first
+    std::vector<int> order;                  // probs[i] is problem order[i]
+    BatchProblem *d_probs = nullptr;
+    void *ws = nullptr;                      // per-slot workspaces
+    size_t ws_stride = 0, vec_stride = 0;
+    int *counter = nullptr;                  // work queue heads, one per time index
+    double *F = nullptr;                     // [nprob][ntimes][2]
+    int *applies = nullptr;                  // [nprob][ntimes]
+    unsigned *err = nullptr;
+    int ntimes_cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<double> graph_times;
+};
+
+// Problem p: len[p] qubits, nterms[p] terms (bits, coeff as for rp_ham_create),
+// W and V single strings, psi0[p] a device complex64 vector, tile[p] the tile
+// exponent (8..12, 0 = default).
+void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms,
+                 const uint64_t *const *bits, const double *const *coeff, const uint64_t *wbits,
+                 const double *wcoeff, const uint64_t *vbits, const double *vcoeff,
+                 const void *const *psi0, const int *tile, int krydim, double tol,
+                 int max_restarts, cudaStream_t st);
+void batch_free(BatchPlan &bp);
+
+// F[p][k] = <psi0| W(t_k) V W(t_k) V |psi0> for every problem; one persistent
+// launch per time step, captured once into a CUDA graph when use_graph.
+void batch_otoc(BatchPlan &bp, int ntimes, const double *times, double *F_host,
+                int *applies_host, int use_graph, cudaStream_t st);
+
+}  // namespace rp

@@ -5,11 +5,16 @@
 
 #include "../../include/rpb200.h"
 #include "rp_apply.cuh"
+#include "rp_batch.cuh"
 #include "rp_krylov.cuh"
 #include "rp_vec.cuh"
 
 struct rp_ham {
     rp::ApplyPlan plan;
+};
+
+struct rp_batch {
+    rp::BatchPlan plan;
 };
 
 namespace rp {
@@ -342,6 +347,44 @@ int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double t
             stats->breakdown = S.breakdown;
             stats->last_err = S.last_err;
         }
+    });
+}
+
+int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nterms,
+                    const uint64_t *const *bits, const double *const *coeff,
+                    const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
+                    const double *vcoeff, const void *const *psi0, const int *tile, int krydim,
+                    double tol, int max_restarts) {
+    return guarded([&] {
+        RP_REQUIRE(b && len && nterms && bits && coeff && wbits && wcoeff && vbits && vcoeff &&
+                       psi0,
+                   RP_E_INVALID, "null argument");
+        rp_batch *B = new rp_batch;
+        try {
+            batch_build(B->plan, nprob, len, nterms, bits, coeff, wbits, wcoeff, vbits, vcoeff,
+                        psi0, tile, krydim, tol, max_restarts, g_stream);
+        } catch (...) {
+            delete B;
+            throw;
+        }
+        *b = B;
+    });
+}
+
+int rp_batch_otoc(rp_batch_t b, int ntimes, const double *times, double *F, int *applies,
+                  int use_graph) {
+    return guarded([&] {
+        RP_REQUIRE(b && times, RP_E_INVALID, "null argument");
+        batch_otoc(b->plan, ntimes, times, F, applies, use_graph, g_stream);
+    });
+}
+
+int rp_batch_destroy(rp_batch_t b) {
+    return guarded([&] {
+        if (!b) return;
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+        batch_free(b->plan);
+        delete b;
     });
 }
 

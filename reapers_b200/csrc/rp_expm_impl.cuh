@@ -8,18 +8,18 @@
 namespace rp {
 
 // Pade numerator coefficients b_0..b_m of Higham (2005), Table 2.2.
-__constant__ double c_b13[14] = {
+static __constant__ double c_b13[14] = {
     64764752532480000.0, 32382376266240000.0, 7771770303897600.0, 1187353796428800.0,
     129060195264000.0,   10559470521600.0,    670442572800.0,     33522128640.0,
     1323241920.0,        40840800.0,          960960.0,           16380.0,
     182.0,               1.0};
-__constant__ double c_b9[10] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0,
+static __constant__ double c_b9[10] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0,
                                 30270240.0,    2162160.0,    110880.0,     3960.0,
                                 90.0,          1.0};
-__constant__ double c_b7[8] = {17297280.0, 8648640.0, 1995840.0, 277200.0,
+static __constant__ double c_b7[8] = {17297280.0, 8648640.0, 1995840.0, 277200.0,
                                25200.0,    1512.0,    56.0,      1.0};
-__constant__ double c_b5[6] = {30240.0, 15120.0, 3360.0, 420.0, 30.0, 1.0};
-__constant__ double c_b3[4] = {120.0, 60.0, 12.0, 1.0};
+static __constant__ double c_b5[6] = {30240.0, 15120.0, 3360.0, 420.0, 30.0, 1.0};
+static __constant__ double c_b3[4] = {120.0, 60.0, 12.0, 1.0};
 
 // C = A * B (n x n), block-wide.
 __device__ static void mm(int n, const cd *A, const cd *B, cd *C) {

@@ -1,0 +1,67 @@
+"""Batched OTOC (one persistent launch per time step, uneven qubit counts)
+against the FP64 CPU oracle and the single-problem mixed path.
+
+Tolerance: 2e-5 absolute on the OTOC (|F(0)| = 1/4), the FP32 state storage
+of the batched form; graph replay and direct launches agree exactly."""
+import numpy as np
+import pytest
+import torch
+
+import reapers_b200 as rb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def make_problems(specs, seed=0):
+    probs, ref_inputs = [], []
+    for i, (N, k) in enumerate(specs):
+        L = N // 2
+        bits, coeff = rb.syk.sparse_syk(N, k=k, seed=seed + i)
+        mb, mc = rb.syk.majoranas(N)
+        rng = np.random.default_rng(100 + i)
+        psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+        psi /= np.linalg.norm(psi)
+        psi32 = psi.astype(np.complex64)
+        w = (mb[N - 1:N], mc[N - 1:N])
+        v = (mb[N - 2:N - 1], mc[N - 2:N - 1])
+        probs.append(dict(len=L, bits=bits, coeff=coeff, w=w, v=v,
+                          psi0=torch.from_numpy(psi32).cuda()))
+        ref_inputs.append((L, bits, coeff, w, v, psi32.astype(np.complex128)))
+    return probs, ref_inputs
+
+
+def test_batched_otoc_matches_oracle_uneven_sizes(cuda):
+    specs = [(16, 4), (18, 4), (20, 4), (16, 4)]
+    probs, refs = make_problems(specs)
+    times = np.array([0.0, 0.6, 1.4])
+    b = rb.BatchOTOC(probs, krydim=10, tol=1e-7, max_restarts=16)
+    F, ap = b.run(times, use_graph=True)
+    F2, ap2 = b.run(times, use_graph=False)
+    assert np.array_equal(F, F2) and np.array_equal(ap, ap2)
+    for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
+        ref = O.otoc(L, bits, coeff, w, v, psi, times, 10, 1e-12)
+        assert np.abs(F[p] - ref).max() < 2e-5, (p, F[p], ref)
+        assert ap[p, 0] == 0 and ap[p, 1] > 0
+
+
+def test_batched_matches_single_problem_mixed_path(cuda):
+    specs = [(18, 8)]
+    probs, refs = make_problems(specs, seed=5)
+    times = np.array([0.9])
+    b = rb.BatchOTOC(probs, krydim=12, tol=1e-7, max_restarts=16)
+    F, ap = b.run(times)
+    L, bits, coeff, w, v, psi = refs[0]
+    ham = rb.Hamiltonian(L, bits, coeff, "c64")
+    wh = rb.Hamiltonian(L, *w, "c64")
+    vh = rb.Hamiltonian(L, *v, "c64")
+    vals, applies = rb.otoc(ham, wh, vh, probs[0]["psi0"], times, 12, 1e-7)
+    assert abs(F[0, 0] - vals[0]) < 2e-5
+    assert abs(int(ap[0, 0]) - applies) <= 12   # same algorithm; rounding may move a pass
+
+
+def test_batched_rejects_bad_tile(cuda):
+    probs, _ = make_problems([(16, 4)])
+    probs[0]["tile"] = 12
+    with pytest.raises(rb.RPError):
+        rb.BatchOTOC(probs)
