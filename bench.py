@@ -195,6 +195,79 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
     return out
 
 
+def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
+              seq_per_size=2, tune=True):
+    """C3 sample: batched OTOC of nreal disorder realisations x nstates random
+    states, sparse SYK k = 8 with N cycling over `sizes` (16/18/20 qubits),
+    t = the first `npts` non-zero points of 40 on [0, 20], m = krydim; one
+    persistent launch per time step in a CUDA graph, tile exponents from the
+    autotuner.  Compared with the same problems run one at a time through the
+    single-problem mixed path (rp_evolve), on seq_per_size problems per size."""
+    import torch
+    import reapers_b200 as rb
+    from reapers_b200 import autotune
+    grid = np.linspace(0.0, 20.0, 40)
+    times = np.array(list(grid[1:1 + npts]))
+    problems = []
+    for r in range(nreal):
+        N = sizes[r % len(sizes)]
+        L = N // 2
+        bits, coeff = rb.syk.sparse_syk(N, k=8, seed=seed * 100003 + r)
+        mb, mc = rb.syk.majoranas(N)
+        for s in range(nstates):
+            psi = rb.random_state(L, "c64", seed=seed * 7919 + r * 64 + s, normalize=True)
+            problems.append(dict(len=L, bits=bits, coeff=coeff, w=(mb[N - 1:N], mc[N - 1:N]),
+                                 v=(mb[N - 2:N - 1], mc[N - 2:N - 1]), psi0=psi, N=N))
+    tol = float(np.finfo(np.float32).eps)
+    tuned = autotune.tune(problems, krydim=krydim, tol=tol) if tune else {}
+    out = {"workload": f"{nreal} sparse-SYK realisations (k=8, N cycling {list(sizes)}) x "
+                       f"{nstates} states = {len(problems)} problems, t in "
+                       f"{[float(round(t, 4)) for t in times]} of 40 points on [0, 20], m={krydim}",
+           "tiles": {k: v["tile"] for k, v in tuned.items()}, "per_size": {}}
+    tot_batch = tot_seq = tot_best = 0.0
+    err = 0.0
+    for N in sizes:
+        idx = [i for i, p in enumerate(problems) if p["N"] == N]
+        sub = [problems[i] for i in idx]
+        b = rb.BatchOTOC(sub, krydim=krydim, tol=tol, max_restarts=16)
+        b.run(times[:1], use_graph=True)    # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        F, ap = b.run(times, use_graph=True)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        b.close()
+        # the same problems one at a time through the single-problem path
+        t0 = time.perf_counter()
+        for j in range(min(seq_per_size, len(sub))):
+            p = sub[j]
+            ham = rb.Hamiltonian(p["len"], p["bits"], p["coeff"], "c64")
+            w = rb.Hamiltonian(p["len"], *p["w"], "c64")
+            v = rb.Hamiltonian(p["len"], *p["v"], "c64")
+            vals, _ = rb.otoc(ham, w, v, p["psi0"], times, krydim, tol)
+            err = max(err, float(np.abs(vals - F[j]).max()))
+        torch.cuda.synchronize()
+        el2 = time.perf_counter() - t0
+        pts = len(sub) * len(times)
+        r_b = pts / el
+        r_s = min(seq_per_size, len(sub)) * len(times) / el2
+        out["per_size"][f"N{N}"] = {"problems": len(sub), "batched_pts_per_s": round(r_b, 3),
+                                    "sequential_pts_per_s": round(r_s, 3),
+                                    "batched_applies": int(ap.sum())}
+        tot_batch += pts / r_b
+        tot_seq += pts / r_s
+        tot_best += pts / max(r_b, r_s)
+    pts = len(problems) * len(times)
+    out["batched_pts_per_s"] = round(pts / tot_batch, 3)
+    out["sequential_pts_per_s"] = round(pts / tot_seq, 3)
+    out["per_size_best_pts_per_s"] = round(pts / tot_best, 3)
+    out["speedup_batched_vs_sequential"] = round(tot_seq / tot_batch, 3)
+    out["max_abs_diff_batched_vs_sequential"] = err
+    out["launches_per_time_step"] = 1
+    out["cuda_graph"] = True
+    return out
+
+
 def make_terms(cfg, seed):
     import reapers_b200 as rb
     return rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed)
@@ -367,6 +440,8 @@ def run_ours(args):
         del x, y, ham
         torch.cuda.empty_cache()
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
+    if args.config == "c4" and not args.no_batch:
+        line["otoc_batched_c3"] = batch_leg(seed=rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
@@ -443,6 +518,7 @@ def main():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c4")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched C3 OTOC leg")
     ap.add_argument("--otoc-points", type=int, default=2,
                     help="non-zero time points of the C4 grid in the OTOC sample")
     ap.add_argument("--profile", action="store_true",

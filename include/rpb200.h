@@ -169,6 +169,9 @@ int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nte
  * captured once into a CUDA graph and replayed. */
 int rp_batch_otoc(rp_batch_t b, int ntimes, const double *times, double *F, int *applies,
                   int use_graph);
+/* One persistent launch doing only napplies H.psi products per problem (no
+ * Krylov); *ms = its device time.  Used by the tile autotuner. */
+int rp_batch_probe(rp_batch_t b, int napplies, double *ms);
 int rp_batch_destroy(rp_batch_t b);
 
 #ifdef __cplusplus

@@ -228,6 +228,12 @@ class BatchOTOC:
                   ap.ctypes.data_as(C.POINTER(C.c_int)), 1 if use_graph else 0)
         return F.view(np.complex128).reshape(self.n, k), ap.reshape(self.n, k)
 
+    def probe(self, napplies=2):
+        """Device ms of one launch doing napplies H.psi products per problem."""
+        ms = C.c_double()
+        _lib.call("rp_batch_probe", self._h, int(napplies), C.byref(ms))
+        return ms.value
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().rp_batch_destroy(self._h)

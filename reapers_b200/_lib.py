@@ -77,6 +77,7 @@ _SIGS = {
                                   C.c_int, C.c_double, C.c_int]),
     "rp_batch_otoc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int), C.c_int]),
+    "rp_batch_probe": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
     "rp_batch_destroy": (C.c_int, [_VP]),
 }
 

@@ -29,6 +29,7 @@ constexpr int BMAXK = 32;        // largest krydim of the batched form
 struct BatchArgs {
     const BatchProblem *probs;
     int nprob, krydim, max_restarts, ti, ntimes, hcap;
+    int probe;          // > 0: only `probe` H.psi products per item (tuning)
     double t, tol;
     double *F;
     int *applies;
@@ -362,6 +363,15 @@ __device__ __noinline__ bool cta_otoc(const BatchProblem &P, const BatchArgs &a,
     Cplx<float> *psi = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 2) * a.vec_stride);
     Cplx<float> *tmp = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 3) * a.vec_stride);
     const double t = a.t;
+    if (a.probe > 0) {   // tuning: H.psi products only
+        cta_copy(psi, P.psi0, n);
+        for (int r = 0; r < a.probe; r++) {
+            if (!cta_apply<B>(P, (r & 1) ? tmp : psi, (r & 1) ? psi : tmp, 1.0, stages, full, git, a.err))
+                return false;
+            applies++;
+        }
+        return true;
+    }
     cta_string(P.vx, P.vz, P.vcr, P.vci, P.psi0, psi, n);
     if (!cta_evolve<B>(P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
     cta_string(P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
@@ -519,6 +529,53 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
     RP_CUDA(cudaMalloc((void **)&bp.err, sizeof(unsigned)));
     RP_CUDA(cudaMemset(bp.err, 0, sizeof(unsigned)));
     (void)st;
+}
+
+double batch_probe(BatchPlan &bp, int napplies, cudaStream_t st) {
+    RP_REQUIRE(napplies >= 1 && napplies <= 64, -2, "napplies must be in [1, 64]");
+    const double zero = 0.0;
+    BatchArgs a{};
+    if (bp.ntimes_cap < 1) {
+        RP_CUDA(cudaMalloc((void **)&bp.counter, sizeof(int)));
+        RP_CUDA(cudaMalloc((void **)&bp.F, (size_t)bp.nprob * 2 * sizeof(double)));
+        RP_CUDA(cudaMalloc((void **)&bp.applies, (size_t)bp.nprob * sizeof(int)));
+        bp.ntimes_cap = 1;
+    }
+    a.probs = bp.d_probs;
+    a.nprob = bp.nprob;
+    a.krydim = bp.krydim;
+    a.max_restarts = bp.max_restarts;
+    a.ntimes = 1;
+    a.hcap = bp.hcap;
+    a.tol = bp.tol;
+    a.t = zero;
+    a.probe = napplies;
+    a.F = bp.F;
+    a.applies = bp.applies;
+    a.ws = static_cast<char *>(bp.ws);
+    a.ws_stride = bp.ws_stride;
+    a.vec_stride = bp.vec_stride;
+    a.counter = bp.counter;
+    a.err = bp.err;
+    const size_t smem = dyn_smem(bp.maxB, bp.hcap);
+    cudaEvent_t e0, e1;
+    RP_CUDA(cudaEventCreate(&e0));
+    RP_CUDA(cudaEventCreate(&e1));
+    RP_CUDA(cudaMemsetAsync(bp.err, 0, sizeof(unsigned), st));
+    RP_CUDA(cudaMemsetAsync(bp.counter, 0, sizeof(int), st));
+    RP_CUDA(cudaEventRecord(e0, st));
+    k_batch_otoc<<<bp.nslots, BT, smem, st>>>(a);
+    RP_CUDA(cudaGetLastError());
+    RP_CUDA(cudaEventRecord(e1, st));
+    unsigned herr = 0;
+    RP_CUDA(cudaMemcpyAsync(&herr, bp.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    RP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RP_REQUIRE(herr == 0, -5, "a device-side wait or bound failed in the batched kernel");
+    return ms;
 }
 
 void batch_otoc(BatchPlan &bp, int ntimes, const double *times, double *F_host,

@@ -52,4 +52,8 @@ void batch_free(BatchPlan &bp);
 void batch_otoc(BatchPlan &bp, int ntimes, const double *times, double *F_host,
                 int *applies_host, int use_graph, cudaStream_t st);
 
+// One launch of `napplies` H.psi products per problem (no Krylov); returns
+// the device time in ms.  Used to tune the tile exponents.
+double batch_probe(BatchPlan &bp, int napplies, cudaStream_t st);
+
 }  // namespace rp

@@ -379,6 +379,13 @@ int rp_batch_otoc(rp_batch_t b, int ntimes, const double *times, double *F, int 
     });
 }
 
+int rp_batch_probe(rp_batch_t b, int napplies, double *ms) {
+    return guarded([&] {
+        RP_REQUIRE(b && ms, RP_E_INVALID, "null argument");
+        *ms = batch_probe(b->plan, napplies, g_stream);
+    });
+}
+
 int rp_batch_destroy(rp_batch_t b) {
     return guarded([&] {
         if (!b) return;

@@ -13,6 +13,7 @@ Majoranas follow the non-block Jordan-Wigner form of FermionOpNonBlockForm
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -99,10 +100,17 @@ def quartic_terms(N, quartets, couplings):
     return bits, coeff
 
 
+@functools.lru_cache(maxsize=8)
+def _all_quartets(N):
+    out = [(i, j, k, l) for i in range(N) for j in range(i) for k in range(j) for l in range(k)]
+    a = np.array(out, dtype=np.int64).reshape(-1, 4)
+    a.setflags(write=False)
+    return a
+
+
 def all_quartets(N):
     """Quartets i > j > k > l in gen_ham's loop order (i outermost)."""
-    out = [(i, j, k, l) for i in range(N) for j in range(i) for k in range(j) for l in range(k)]
-    return np.array(out, dtype=np.int64).reshape(-1, 4)
+    return _all_quartets(N)
 
 
 def _unrank_quartets(N, ranks):
