@@ -268,6 +268,72 @@ def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40)
     return out
 
 
+def step_leg(T=10.0, tol=1e-8, seed=0):
+    """C5: learned (dt, m) step controller vs Expokit's plain step control at
+    equal tolerance, on XXZ L=24 (J = Jz = 1, fields U[-W, W], W in {0.5, 3})
+    and sparse SYK N=48 (k=8), FP64, exp(-iHT) psi with T = 10.  The network
+    is the committed model (trained on the GPU on plain-method traces of
+    smaller problems, reapers_b200/data); without it a small model is trained
+    here first and the line says so."""
+    import torch
+    import reapers_b200 as rb
+    from reapers_b200 import stepper as SP
+    out = {"workload": f"exp(-iHT)psi, T={T}, tol={tol}, FP64; plain = Expokit step control "
+                       f"with m=30; learned = MLP-proposed (dt, m), m in [{SP.M_MIN}, {SP.M_MAX}]",
+           "problems": {}}
+    if os.path.exists(SP.DEFAULT_MODEL):
+        model = SP.StepModel.load()
+        out["model"] = dict(model.meta, source="committed")
+    else:
+        t0 = time.perf_counter()
+        runs = []
+        for p in SP.training_problems(60, seed=seed + 1):
+            runs.extend(SP.generate_traces([p]))
+            p["ham"].close()
+        X, Y = SP.make_dataset(runs)
+        model, loss = SP.train(X, Y, epochs=40)
+        out["model"] = dict(model.meta, source="trained in this run",
+                            seconds=round(time.perf_counter() - t0, 2))
+    rng = np.random.default_rng(seed + 2024)
+    cases = [("xxz_L24_W0.5", 24, rb.syk.xxz_chain(24, 1.0, rng.uniform(-0.5, 0.5, 24))),
+             ("xxz_L24_W3", 24, rb.syk.xxz_chain(24, 1.0, rng.uniform(-3.0, 3.0, 24))),
+             ("sparse_syk_N48", 24, rb.syk.sparse_syk(48, k=8, seed=seed + 1000))]
+    tot = {"plain": [0, 0.0], "learned": [0, 0.0]}
+    for name, L, (bits, coeff) in cases:
+        ham = rb.Hamiltonian(L, bits, coeff, "c128")
+        psi = rb.random_state(L, "c128", seed=seed + 11)
+        # warm-up: one small step of each basis size range
+        SP.step_evolve(ham, psi.clone(), 1e-3, tol, SP.PlainController(30))
+        res, finals = {}, {}
+        for ctl in (SP.PlainController(30), SP.LearnedController(model)):
+            ps = psi.clone()
+            st = SP.step_evolve(ham, ps, T, tol, ctl)
+            st.pop("trace", None)
+            rec = {"steps": st["steps"], "applies": st["applies"],
+                   "seconds": round(st["seconds"], 4), "rejections": st["rejections"],
+                   "err_estimate_sum": st["err_sum"], "modelled_vector_passes": st["cost"]}
+            if ctl.name == "learned":
+                rec["proposals"] = st["proposals"]
+                rec["accepted_fraction"] = round(st["proposals_accepted"] / max(1, st["proposals"]), 4)
+                rec["ms_in_mlp"] = round(st["ms_mlp"], 3)
+            res[ctl.name] = rec
+            finals[ctl.name] = ps
+            tot[ctl.name][0] += st["applies"]
+            tot[ctl.name][1] += st["seconds"]
+        res["final_state_diff"] = float(torch.linalg.vector_norm(finals["plain"] -
+                                                                 finals["learned"]).item())
+        res["speedup_wall"] = round(res["plain"]["seconds"] / res["learned"]["seconds"], 3)
+        res["applies_ratio"] = round(res["learned"]["applies"] / res["plain"]["applies"], 3)
+        out["problems"][name] = res
+        del finals, psi
+        ham.close()
+        torch.cuda.empty_cache()
+    model.close()
+    out["total_applies"] = {"plain": tot["plain"][0], "learned": tot["learned"][0]}
+    out["speedup_wall_total"] = round(tot["plain"][1] / tot["learned"][1], 3)
+    return out
+
+
 def make_terms(cfg, seed):
     import reapers_b200 as rb
     return rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed)
@@ -442,6 +508,8 @@ def run_ours(args):
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
     if args.config == "c4" and not args.no_batch:
         line["otoc_batched_c3"] = batch_leg(seed=rank)
+    if args.config == "c4" and not args.no_steps:
+        line["learned_steps_c5"] = step_leg(seed=rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
@@ -519,6 +587,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched C3 OTOC leg")
+    ap.add_argument("--no-steps", action="store_true",
+                    help="skip the learned step-controller C5 leg")
     ap.add_argument("--otoc-points", type=int, default=2,
                     help="non-zero time points of the C4 grid in the OTOC sample")
     ap.add_argument("--profile", action="store_true",

@@ -147,6 +147,48 @@ int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double t
 /* Free the cached Krylov workspace (krydim + 2 vectors). */
 int rp_workspace_release(void);
 
+/* --- time-stepped Krylov primitives (no reference counterpart: the
+ * reference only has the restarted evolve; these let a step controller
+ * advance exp(-i dt H) psi one sub-step at a time) ------------------------ */
+typedef struct {
+    int m_eff;           /* basis size (m unless an invariant subspace was found) */
+    int breakdown;
+    int passes;          /* orthogonalisation passes taken (1 to 3 per basis vector) */
+    int pad;
+    double beta;         /* h_{m+1,m}: norm of the last orthogonalised vector */
+    double beta0;        /* ||psi|| */
+} rp_arnoldi_info_t;
+/* One Arnoldi cycle of psi with m basis vectors (the reference's
+ * orthogonalisation, inc/algo.h:77-173); the basis stays on the device until
+ * the next call.  H receives the m x m Hessenberg matrix, complex interleaved,
+ * column-major (2*m*m doubles). */
+int rp_arnoldi(rp_ham_t h, const void *psi, int m, double *H, rp_arnoldi_info_t *info);
+/* out = sum_{i < m_eff} coef_i v_i over the last rp_arnoldi basis
+ * (coef: 2*m_eff doubles, complex interleaved). */
+int rp_arnoldi_combine(const double *coef, void *out);
+/* For c < ncand: col0[c] = first column of exp((fr[c] + i fi[c]) H), H m x m
+ * complex column-major; FP64 Pade-13 on the GPU, one CTA per candidate
+ * (col0: 2*m*ncand doubles). */
+int rp_expm_first_column(int m, const double *H, int ncand, const double *fr, const double *fi,
+                         double *col0);
+
+/* --- MLP of the learned step controller (no reference counterpart) -------
+ * in -> 64 -> 64 -> out, tanh hidden layers, FP32; forward, backward and
+ * Adam are CUDA kernels.  Arrays are host row-major [n][in] / [n][out]. */
+typedef struct rp_mlp *rp_mlp_t;
+int rp_mlp_create(rp_mlp_t *net, int in_dim, int out_dim, uint64_t seed);
+int rp_mlp_num_params(rp_mlp_t net, int *n);
+/* flat parameters [W1 (64 x in), b1, W2 (64 x 64), b2, W3 (out x 64), b3] */
+int rp_mlp_get_params(rp_mlp_t net, float *p);
+int rp_mlp_set_params(rp_mlp_t net, const float *p);
+int rp_mlp_forward(rp_mlp_t net, const float *X, int n, float *Y);
+/* mean loss (1/2 squared error) and its gradient over n samples */
+int rp_mlp_grad(rp_mlp_t net, const float *X, const float *Y, int n, float *grad, float *loss);
+/* Adam over shuffled mini-batches; *loss = mean loss of the last epoch */
+int rp_mlp_train(rp_mlp_t net, const float *X, const float *Y, int n, int epochs, int batch,
+                 float lr, uint64_t seed, float *loss);
+int rp_mlp_destroy(rp_mlp_t net);
+
 /* --- batched OTOC (the outer loops of examples/syk.cc:417-475 and
  * examples/simple-syk-krylov.cc:42-57 over many disorder realisations and
  * states, run as one persistent launch per time step) ---------------------- */

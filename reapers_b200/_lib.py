@@ -38,6 +38,12 @@ class EvolveStats(C.Structure):
                 ("prods", C.c_int), ("breakdown", C.c_int), ("last_err", C.c_double)]
 
 
+class ArnoldiInfo(C.Structure):
+    _fields_ = [("m_eff", C.c_int), ("breakdown", C.c_int), ("passes", C.c_int),
+                ("pad", C.c_int), ("beta", C.c_double),
+                ("beta0", C.c_double)]
+
+
 # name -> (restype, argtypes); every exported symbol of include/rpb200.h
 _VP = C.c_void_p
 _SIGS = {
@@ -69,6 +75,21 @@ _SIGS = {
     "rp_evolve": (C.c_int, [_VP, _VP, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                             C.POINTER(EvolveStats)]),
     "rp_workspace_release": (C.c_int, []),
+    "rp_arnoldi": (C.c_int, [_VP, _VP, C.c_int, C.POINTER(C.c_double), C.POINTER(ArnoldiInfo)]),
+    "rp_arnoldi_combine": (C.c_int, [C.POINTER(C.c_double), _VP]),
+    "rp_expm_first_column": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]),
+    "rp_mlp_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, C.c_uint64]),
+    "rp_mlp_num_params": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "rp_mlp_get_params": (C.c_int, [_VP, C.POINTER(C.c_float)]),
+    "rp_mlp_set_params": (C.c_int, [_VP, C.POINTER(C.c_float)]),
+    "rp_mlp_forward": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float)]),
+    "rp_mlp_grad": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                              C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "rp_mlp_train": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int,
+                               C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "rp_mlp_destroy": (C.c_int, [_VP]),
     "rp_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(C.c_int),
                                   C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint64)),
                                   C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_uint64),

@@ -7,6 +7,7 @@
 #include "rp_apply.cuh"
 #include "rp_batch.cuh"
 #include "rp_krylov.cuh"
+#include "rp_mlp.cuh"
 #include "rp_vec.cuh"
 
 struct rp_ham {
@@ -17,12 +18,17 @@ struct rp_batch {
     rp::BatchPlan plan;
 };
 
+struct rp_mlp {
+    rp::Mlp net;
+};
+
 namespace rp {
 
 static thread_local std::string g_err = "no error";
 static cudaStream_t g_stream = nullptr;
 static int g_device = -1;
 static KryWorkspace g_ws;
+static ArnoldiResult g_arn;   // the basis of the last rp_arnoldi
 static std::mutex g_mu;
 
 void set_error(int code, const std::string &msg) {
@@ -347,6 +353,103 @@ int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double t
             stats->breakdown = S.breakdown;
             stats->last_err = S.last_err;
         }
+    });
+}
+
+int rp_arnoldi(rp_ham_t h, const void *psi, int m, double *H, rp_arnoldi_info_t *info) {
+    return guarded([&] {
+        RP_REQUIRE(h && H && info, RP_E_INVALID, "null argument");
+        check_vec(psi);
+        krylov_arnoldi(h->plan, g_ws, psi, m, g_arn, g_stream);
+        std::copy(g_arn.H.begin(), g_arn.H.end(), H);
+        info->m_eff = g_arn.m_eff;
+        info->breakdown = g_arn.breakdown;
+        info->passes = g_arn.passes;
+        info->pad = 0;
+        info->beta = g_arn.beta;
+        info->beta0 = g_arn.beta0;
+    });
+}
+
+int rp_arnoldi_combine(const double *coef, void *out) {
+    return guarded([&] {
+        RP_REQUIRE(coef, RP_E_INVALID, "null argument");
+        check_vec(out);
+        krylov_combine(g_ws, g_arn, coef, out, g_stream);
+    });
+}
+
+int rp_expm_first_column(int m, const double *H, int ncand, const double *fr, const double *fi,
+                         double *col0) {
+    return guarded([&] {
+        RP_REQUIRE(H && fr && fi && col0, RP_E_INVALID, "null argument");
+        expm_candidates(m, H, ncand, fr, fi, col0, g_stream);
+    });
+}
+
+int rp_mlp_create(rp_mlp_t *net, int in_dim, int out_dim, uint64_t seed) {
+    return guarded([&] {
+        RP_REQUIRE(net, RP_E_INVALID, "null argument");
+        rp_mlp *M = new rp_mlp;
+        try {
+            mlp_create(M->net, in_dim, out_dim, seed);
+        } catch (...) {
+            mlp_free(M->net);
+            delete M;
+            throw;
+        }
+        *net = M;
+    });
+}
+
+int rp_mlp_num_params(rp_mlp_t net, int *n) {
+    return guarded([&] {
+        RP_REQUIRE(net && n, RP_E_INVALID, "null argument");
+        *n = net->net.np;
+    });
+}
+
+int rp_mlp_get_params(rp_mlp_t net, float *p) {
+    return guarded([&] {
+        RP_REQUIRE(net && p, RP_E_INVALID, "null argument");
+        mlp_get(net->net, p);
+    });
+}
+
+int rp_mlp_set_params(rp_mlp_t net, const float *p) {
+    return guarded([&] {
+        RP_REQUIRE(net && p, RP_E_INVALID, "null argument");
+        mlp_set(net->net, p);
+    });
+}
+
+int rp_mlp_forward(rp_mlp_t net, const float *X, int n, float *Y) {
+    return guarded([&] {
+        RP_REQUIRE(net && X && Y && n >= 0, RP_E_INVALID, "bad argument");
+        if (n) mlp_forward(net->net, X, n, Y, g_stream);
+    });
+}
+
+int rp_mlp_grad(rp_mlp_t net, const float *X, const float *Y, int n, float *grad, float *loss) {
+    return guarded([&] {
+        RP_REQUIRE(net && X && Y && grad && loss, RP_E_INVALID, "null argument");
+        *loss = mlp_grad(net->net, X, Y, n, grad, g_stream);
+    });
+}
+
+int rp_mlp_train(rp_mlp_t net, const float *X, const float *Y, int n, int epochs, int batch,
+                 float lr, uint64_t seed, float *loss) {
+    return guarded([&] {
+        RP_REQUIRE(net && X && Y && loss, RP_E_INVALID, "null argument");
+        *loss = mlp_train(net->net, X, Y, n, epochs, batch, lr, seed, g_stream);
+    });
+}
+
+int rp_mlp_destroy(rp_mlp_t net) {
+    return guarded([&] {
+        if (!net) return;
+        mlp_free(net->net);
+        delete net;
     });
 }
 

@@ -20,6 +20,7 @@
 // both vector precisions.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "rp_expm_impl.cuh"
@@ -28,6 +29,21 @@
 namespace rp {
 
 static size_t esize(int dtype) { return dtype == 2 ? 16 : 8; }
+
+// The first orthogonalisation pass's projections <v_i|w> can be taken in the
+// H.psi kernel's epilogue (w never leaves the SM before it is projected) or by
+// the grouped projection kernel after the apply.  The separate kernel streams
+// the basis at a higher fraction of HBM bandwidth than the epilogue, whose
+// per-row warp reductions slow the apply, so it is the default;
+// RPB200_FUSED_DOTS=1 selects the fused form.
+static bool fused_projections() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("RPB200_FUSED_DOTS");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
 
 static void grow_hfull(KryWorkspace &ws, int need, cudaStream_t st) {
     if (need <= ws.hcap) return;
@@ -60,6 +76,7 @@ void workspace_release(KryWorkspace &ws) {
     if (ws.hfull) cudaFree(ws.hfull);
     if (ws.escratch) cudaFree(ws.escratch);
     if (ws.err) cudaFree(ws.err);
+    if (ws.tab) cudaFree(ws.tab);
     ws = KryWorkspace{};
 }
 
@@ -81,6 +98,7 @@ void workspace_ensure(KryWorkspace &ws, int len, int dtype, int krydim) {
         RP_CUDA(cudaMalloc((void **)&ws.norm_partials, (size_t)g * sizeof(double)));
         RP_CUDA(cudaMalloc((void **)&ws.err, sizeof(unsigned)));
         RP_CUDA(cudaMemset(ws.err, 0, sizeof(unsigned)));
+        RP_CUDA(cudaMalloc((void **)&ws.tab, (MAX_KRYLOV + 1) * sizeof(void *)));
     } catch (Error &e) {
         workspace_release(ws);
         throw Error{-4, "device out of memory for the Krylov workspace (" + e.msg + ")"};
@@ -275,14 +293,9 @@ void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_
     RP_CUDA(cudaGetLastError());
 
     // device copy of the pointer table for the fused projections of the apply
-    void **d_tab = nullptr;
-    RP_CUDA(cudaMalloc((void **)&d_tab, (MAX_KRYLOV + 1) * sizeof(void *)));
-    struct TabGuard {
-        void **p;
-        ~TabGuard() { cudaFree(p); }
-    } guard{d_tab};
+    void **d_tab = ws.tab;
 
-    const bool fused = !plan.cfg.direct;
+    const bool fused = !plan.cfg.direct && fused_projections();
     const int agrid = fused ? apply_grid(plan) : reduce_grid();
     const int rgrid = reduce_grid();
     KryDev *s = ws.dev;
@@ -350,6 +363,142 @@ void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_
     RP_CUDA(cudaMemcpyAsync(psi, ws.y, D * esize(dtype), cudaMemcpyDeviceToDevice, st));
     RP_CUDA(cudaStreamSynchronize(st));
     if (stats) *stats = S;
+}
+
+// ---------------------------------------------------------------------------
+// Time-stepped primitives
+// ---------------------------------------------------------------------------
+void krylov_arnoldi(const ApplyPlan &plan, KryWorkspace &ws, const void *psi, int m,
+                    ArnoldiResult &R, cudaStream_t st) {
+    RP_REQUIRE(m >= 2 && m <= MAX_KRYLOV, -2, "m must be in [2, 64]");
+    // a step controller varies m from step to step: keep a larger basis
+    // allocation instead of reallocating it
+    const bool same = ws.dev && ws.len == plan.len && ws.dtype == plan.dtype;
+    workspace_ensure(ws, plan.len, plan.dtype, same ? std::max(ws.krydim, m) : m);
+    const uint64_t D = ws.D;
+    const int dtype = plan.dtype;
+    R = ArnoldiResult{};
+    R.m = m;
+    R.beta0 = vec_norm_sync(dtype, D, psi, &ws, st);
+    R.H.assign((size_t)2 * m * m, 0.0);
+    R.sigma.assign(m + 1, 0.0);
+    if (R.beta0 == 0.0) return;
+    RP_CUDA(cudaMemcpyAsync(ws.u[0], psi, D * esize(dtype), cudaMemcpyDeviceToDevice, st));
+    RP_CUDA(cudaMemsetAsync(ws.err, 0, sizeof(unsigned), st));
+    k_kry_init<<<1, 32, 0, st>>>(ws.dev, R.beta0);
+    k_kry_begin<<<1, 256, 0, st>>>(ws.dev, m, 0);
+    RP_CUDA(cudaGetLastError());
+    void **d_tab = ws.tab;
+    VecTable tab{};
+    for (int i = 0; i <= m; i++) tab.p[i] = ws.u[i];
+    RP_CUDA(cudaMemcpyAsync(d_tab, tab.p, (m + 1) * sizeof(void *), cudaMemcpyHostToDevice, st));
+    const bool fused = !plan.cfg.direct && fused_projections();
+    const int agrid = fused ? apply_grid(plan) : reduce_grid();
+    const int rgrid = reduce_grid();
+    KryDev *s = ws.dev;
+    for (int j = 0; j < m; j++) {
+        void *w = ws.u[j + 1];
+        ApplyLaunch L;
+        L.in = ws.u[j];
+        L.out = w;
+        L.alpha_dev = &s->sigma[j];
+        L.active = &s->active;
+        L.err = ws.err;
+        if (fused) {
+            L.dot_vecs = (const void *const *)d_tab;
+            L.ndot = j + 1;
+            L.partials = ws.partials;
+            apply_launch(plan, L, st);
+        } else {
+            apply_launch(plan, L, st);
+            multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, nullptr, st);
+        }
+        k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, agrid, j, 1);
+        multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials, &s->active,
+                   nullptr, st);
+        k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, m, 1);
+        for (int pass = 2; pass <= 3; pass++) {
+            multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, &s->again, st);
+            k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, rgrid, j, pass);
+            multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials, &s->active,
+                       &s->again, st);
+            k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, m, pass);
+        }
+    }
+    RP_CUDA(cudaGetLastError());
+    KryHeader hdr{};
+    unsigned herr = 0;
+    RP_CUDA(cudaMemcpyAsync(&hdr, s, sizeof(hdr), cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(R.H.data(), s->H, R.H.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(R.sigma.data(), s->sigma, (m + 1) * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(&herr, ws.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
+    RP_REQUIRE(herr == 0, -5, "a device-side wait timed out in the H.psi kernel");
+    R.m_eff = hdr.m_eff;
+    R.breakdown = hdr.brokedown;
+    R.passes = hdr.passes;
+    R.beta = hdr.beta;
+}
+
+void krylov_combine(KryWorkspace &ws, const ArnoldiResult &R, const double *coef, void *out,
+                    cudaStream_t st) {
+    RP_REQUIRE(R.m_eff >= 1 && (int)ws.u.size() >= R.m_eff, -2, "no Arnoldi basis to combine");
+    std::vector<double> c((size_t)2 * R.m_eff);
+    for (int i = 0; i < R.m_eff; i++) {
+        c[2 * i] = coef[2 * i] * R.sigma[i];
+        c[2 * i + 1] = coef[2 * i + 1] * R.sigma[i];
+    }
+    RP_CUDA(cudaMemcpyAsync(ws.dev->ycoef, c.data(), c.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    RP_CUDA(cudaMemsetAsync(out, 0, ws.D * esize(ws.dtype), st));
+    VecTable tab{};
+    for (int i = 0; i < R.m_eff; i++) tab.p[i] = ws.u[i];
+    multi_axpy(ws.dtype, ws.D, tab, R.m_eff, nullptr, ws.dev->ycoef, out, nullptr, nullptr,
+               nullptr, st);
+    RP_CUDA(cudaStreamSynchronize(st));
+}
+
+__global__ void __launch_bounds__(256) k_expm_cands(int m, const cd *H, const double *fr,
+                                                    const double *fi, cd *scratch, cd *col0) {
+    extern __shared__ double smem[];
+    const int c = blockIdx.x;
+    cd *A = scratch + (size_t)c * 10 * m * m, *E = A + (size_t)m * m, *ws = E + (size_t)m * m;
+    const cd f{fr[c], fi[c]};
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = cmul(f, H[e]);
+    __syncthreads();
+    expm_block(m, A, E, ws, smem);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) col0[(size_t)c * m + i] = E[i];
+}
+
+void expm_candidates(int m, const double *H, int ncand, const double *fr, const double *fi,
+                     double *col0, cudaStream_t st) {
+    RP_REQUIRE(m >= 1 && m <= 256 && ncand >= 1 && ncand <= 64, -2, "bad expm batch size");
+    const size_t hb = (size_t)m * m * sizeof(cd);
+    const size_t sb = (size_t)ncand * 10 * m * m * sizeof(cd);
+    const size_t need = hb + sb + 2 * ncand * sizeof(double) + (size_t)ncand * m * sizeof(cd);
+    // one buffer kept between calls (a step controller calls this every step)
+    static char *buf = nullptr;
+    static size_t cap = 0;
+    if (need > cap) {
+        RP_CUDA(cudaStreamSynchronize(st));
+        if (buf) cudaFree(buf);
+        buf = nullptr;
+        cap = 0;
+        RP_CUDA(cudaMalloc((void **)&buf, need));
+        cap = need;
+    }
+    cd *dH = (cd *)buf;
+    cd *scr = (cd *)(buf + hb);
+    double *dfr = (double *)(buf + hb + sb), *dfi = dfr + ncand;
+    cd *dcol = (cd *)(dfi + ncand);
+    RP_CUDA(cudaMemcpyAsync(dH, H, hb, cudaMemcpyHostToDevice, st));
+    RP_CUDA(cudaMemcpyAsync(dfr, fr, ncand * sizeof(double), cudaMemcpyHostToDevice, st));
+    RP_CUDA(cudaMemcpyAsync(dfi, fi, ncand * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_expm_cands<<<ncand, 256, (size_t)(2 * m + 64) * sizeof(double), st>>>(m, dH, dfr, dfi, scr, dcol);
+    RP_CUDA(cudaGetLastError());
+    RP_CUDA(cudaMemcpyAsync(col0, dcol, (size_t)ncand * m * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace rp

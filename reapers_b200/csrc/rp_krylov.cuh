@@ -51,6 +51,7 @@ struct KryWorkspace {
     void *hfull = nullptr;   // hcap x hcap complex double
     void *escratch = nullptr;
     unsigned *err = nullptr;
+    void **tab = nullptr;    // device copy of the basis pointer table
 };
 
 void workspace_ensure(KryWorkspace &ws, int len, int dtype, int krydim);
@@ -65,5 +66,26 @@ void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_
 
 // sqrt(<v|v>) (compensated FP64), synchronous.
 double vec_norm_sync(int dtype, uint64_t n, const void *v, KryWorkspace *ws, cudaStream_t st);
+
+// --- time-stepped Krylov primitives (used by the step controllers) -------
+// One Arnoldi cycle of psi with m vectors, the reference's orthogonalisation
+// (inc/algo.h:77-173): the basis stays in the workspace; H (m x m complex,
+// column-major), the last norm beta = h_{m+1,m}, beta0 = ||psi|| and the
+// basis scales come back to the host.
+struct ArnoldiResult {
+    int m = 0, m_eff = 0, breakdown = 0, passes = 0;
+    double beta = 0, beta0 = 0;
+    std::vector<double> H;       // 2 * m * m
+    std::vector<double> sigma;   // m + 1
+};
+void krylov_arnoldi(const ApplyPlan &plan, KryWorkspace &ws, const void *psi, int m,
+                    ArnoldiResult &R, cudaStream_t st);
+// out = sum_{i < m_eff} coef_i v_i over the last basis (coef complex, host).
+void krylov_combine(KryWorkspace &ws, const ArnoldiResult &R, const double *coef, void *out,
+                    cudaStream_t st);
+// col0[c] = first column of exp(f_c H) for ncand factors f_c = fr[c] + i fi[c]
+// (FP64 Pade-13 on the GPU, one CTA per candidate).
+void expm_candidates(int m, const double *H, int ncand, const double *fr, const double *fi,
+                     double *col0, cudaStream_t st);
 
 }  // namespace rp

@@ -146,22 +146,129 @@ __device__ __forceinline__ double block_sum(double v, double *scratch) {
     return r;
 }
 
-// Each CTA owns a contiguous chunk of elements.  For every vector u_i it sums
-// conj(u_i) * w over the chunk; w is re-read from L2/L1 per vector.
+// Vectors are streamed as 16-byte packets: one complex double or two complex
+// floats.  A packet count of n * sizeof(element) / 16 requires an even n for
+// complex64; the element-wise kernels further down handle the odd case.
 template <typename Real>
-__global__ void __launch_bounds__(RT) k_multi_dot(uint64_t n, const VecTable tab, int nvec,
-                                                  const Cplx<Real> *w, double *partials,
+struct Packet;
+template <>
+struct Packet<double> {
+    static constexpr int E = 1;
+    double2 v;
+    __device__ __forceinline__ void load(const void *p, uint64_t k) {
+        v = __ldg(static_cast<const double2 *>(p) + k);
+    }
+    __device__ __forceinline__ void load_rw(const void *p, uint64_t k) {
+        v = static_cast<const double2 *>(p)[k];
+    }
+    __device__ __forceinline__ double re(int) const { return v.x; }
+    __device__ __forceinline__ double im(int) const { return v.y; }
+    __device__ __forceinline__ void set(int, double r, double i) { v = make_double2(r, i); }
+    __device__ __forceinline__ void store(void *p, uint64_t k) const {
+        static_cast<double2 *>(p)[k] = v;
+    }
+};
+template <>
+struct Packet<float> {
+    static constexpr int E = 2;
+    float4 v;
+    __device__ __forceinline__ void load(const void *p, uint64_t k) {
+        v = __ldg(static_cast<const float4 *>(p) + k);
+    }
+    __device__ __forceinline__ void load_rw(const void *p, uint64_t k) {
+        v = static_cast<const float4 *>(p)[k];
+    }
+    __device__ __forceinline__ double re(int e) const { return e ? v.z : v.x; }
+    __device__ __forceinline__ double im(int e) const { return e ? v.w : v.y; }
+    __device__ __forceinline__ void set(int e, double r, double i) {
+        if (e) {
+            v.z = (float)r;
+            v.w = (float)i;
+        } else {
+            v.x = (float)r;
+            v.y = (float)i;
+        }
+    }
+    __device__ __forceinline__ void store(void *p, uint64_t k) const {
+        static_cast<float4 *>(p)[k] = v;
+    }
+};
+
+constexpr int DOT_G = 8;   // vectors per group of the projection kernel
+
+// Projections <u_i | w>: each CTA owns a contiguous chunk of packets and
+// takes the vectors in groups of DOT_G, reading w once per group and the
+// group's vectors side by side (DOT_G + 1 independent 16-byte loads in
+// flight per thread).  Per-thread FP64 sums, then a fixed-order compensated
+// combination across the CTA's warps.
+template <typename Real>
+__global__ void __launch_bounds__(RT) k_multi_dot(uint64_t npk, const VecTable tab, int nvec,
+                                                  const void *w, double *partials,
                                                   const int *gate, const int *gate2) {
+    if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
+    constexpr int E = Packet<Real>::E;
+    __shared__ double scratch[RW][2 * DOT_G];
+    const uint64_t chunk = (npk + gridDim.x - 1) / gridDim.x;
+    const uint64_t lo = blockIdx.x * chunk;
+    const uint64_t hi = lo + chunk < npk ? lo + chunk : npk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int g0 = 0; g0 < nvec; g0 += DOT_G) {
+        const int ng = nvec - g0 < DOT_G ? nvec - g0 : DOT_G;
+        double sr[DOT_G], si[DOT_G];
+#pragma unroll
+        for (int q = 0; q < DOT_G; q++) sr[q] = si[q] = 0.0;
+        for (uint64_t k = lo + threadIdx.x; k < hi; k += RT) {
+            Packet<Real> wp, up[DOT_G];
+            wp.load_rw(w, k);
+#pragma unroll
+            for (int q = 0; q < DOT_G; q++)
+                if (q < ng) up[q].load(tab.p[g0 + q], k);
+#pragma unroll
+            for (int q = 0; q < DOT_G; q++) {
+                if (q < ng) {
+#pragma unroll
+                    for (int e = 0; e < E; e++) {
+                        const double ar = up[q].re(e), ai = up[q].im(e);
+                        const double br = wp.re(e), bi = wp.im(e);
+                        sr[q] = fma(ar, br, fma(ai, bi, sr[q]));
+                        si[q] = fma(ar, bi, fma(-ai, br, si[q]));
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < DOT_G; q++) {
+            const double a = warp_sum(sr[q]), b = warp_sum(si[q]);
+            if (lane == 0) {
+                scratch[warp][2 * q] = a;
+                scratch[warp][2 * q + 1] = b;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 2 * ng) {
+            CompSum c;
+            for (int wi = 0; wi < RW; wi++) c.add(scratch[wi][threadIdx.x]);
+            const int q = threadIdx.x >> 1;
+            partials[((size_t)blockIdx.x * nvec + g0 + q) * 2 + (threadIdx.x & 1)] = c.value();
+        }
+        __syncthreads();
+    }
+}
+
+// Element-wise fallback for a complex64 vector of odd length.
+__global__ void __launch_bounds__(RT) k_multi_dot_odd(uint64_t n, const VecTable tab, int nvec,
+                                                      const Cplx<float> *w, double *partials,
+                                                      const int *gate, const int *gate2) {
     if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
     __shared__ double scratch[RW];
     const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
     const uint64_t lo = blockIdx.x * chunk;
     const uint64_t hi = lo + chunk < n ? lo + chunk : n;
     for (int i = 0; i < nvec; i++) {
-        const Cplx<Real> *u = static_cast<const Cplx<Real> *>(tab.p[i]);
+        const Cplx<float> *u = static_cast<const Cplx<float> *>(tab.p[i]);
         double sr = 0.0, si = 0.0;
         for (uint64_t k = lo + threadIdx.x; k < hi; k += RT) {
-            const Cplx<Real> a = u[k], b = w[k];
+            const Cplx<float> a = u[k], b = w[k];
             sr = fma((double)a.x, (double)b.x, fma((double)a.y, (double)b.y, sr));
             si = fma((double)a.x, (double)b.y, fma(-(double)a.y, (double)b.x, si));
         }
@@ -179,17 +286,80 @@ void multi_dot_partials(int dtype, uint64_t n, const VecTable &tab, int nvec, co
     RP_REQUIRE(nvec >= 0 && nvec <= MAX_KRYLOV + 1, -2, "too many vectors");
     const int g = reduce_grid();
     if (dtype == 2)
-        k_multi_dot<double><<<g, RT, 0, st>>>(n, tab, nvec, (const Cplx<double> *)w, partials, gate, gate2);
+        k_multi_dot<double><<<g, RT, 0, st>>>(n, tab, nvec, w, partials, gate, gate2);
+    else if (n % 2 == 0)
+        k_multi_dot<float><<<g, RT, 0, st>>>(n / 2, tab, nvec, w, partials, gate, gate2);
     else
-        k_multi_dot<float><<<g, RT, 0, st>>>(n, tab, nvec, (const Cplx<float> *)w, partials, gate, gate2);
+        k_multi_dot_odd<<<g, RT, 0, st>>>(n, tab, nvec, (const Cplx<float> *)w, partials, gate, gate2);
     RP_CUDA(cudaGetLastError());
 }
 
+constexpr int AXPY_G = 8;   // vectors loaded side by side by the update kernel
+
+// w += sum_i c_i u_i and ||w||^2 in one pass: per packet of w, the vectors
+// are read in groups of AXPY_G independent 16-byte loads, the update is
+// accumulated in FP64 and rounded once to the vector precision.
 template <typename Real>
-__global__ void __launch_bounds__(RT) k_multi_axpy(uint64_t n, const VecTable tab, int nvec,
+__global__ void __launch_bounds__(RT) k_multi_axpy(uint64_t npk, const VecTable tab, int nvec,
                                                    const int *nvec_dev, const double *coef,
-                                                   Cplx<Real> *w, double *norm_partials,
+                                                   void *w, double *norm_partials,
                                                    const int *gate, const int *gate2) {
+    if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
+    constexpr int E = Packet<Real>::E;
+    __shared__ double scratch[RW];
+    __shared__ double c[2 * (MAX_KRYLOV + 1)];
+    const int nv = nvec_dev ? *nvec_dev : nvec;
+    for (int i = threadIdx.x; i < 2 * nv; i += RT) c[i] = coef[i];
+    __syncthreads();
+    const uint64_t chunk = (npk + gridDim.x - 1) / gridDim.x;
+    const uint64_t lo = blockIdx.x * chunk;
+    const uint64_t hi = lo + chunk < npk ? lo + chunk : npk;
+    double nrm = 0.0;
+    for (uint64_t k = lo + threadIdx.x; k < hi; k += RT) {
+        Packet<Real> wp;
+        wp.load_rw(w, k);
+        double xr[E], xi[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            xr[e] = wp.re(e);
+            xi[e] = wp.im(e);
+        }
+        for (int i0 = 0; i0 < nv; i0 += AXPY_G) {
+            Packet<Real> up[AXPY_G];
+#pragma unroll
+            for (int q = 0; q < AXPY_G; q++)
+                if (i0 + q < nv) up[q].load(tab.p[i0 + q], k);
+#pragma unroll
+            for (int q = 0; q < AXPY_G; q++) {
+                if (i0 + q < nv) {
+                    const double cr = c[2 * (i0 + q)], ci = c[2 * (i0 + q) + 1];
+#pragma unroll
+                    for (int e = 0; e < E; e++) {
+                        const double ur = up[q].re(e), ui = up[q].im(e);
+                        xr[e] = fma(cr, ur, fma(-ci, ui, xr[e]));
+                        xi[e] = fma(cr, ui, fma(ci, ur, xi[e]));
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            wp.set(e, xr[e], xi[e]);
+            const double rr = wp.re(e), ri = wp.im(e);   // the rounded values
+            nrm = fma(rr, rr, fma(ri, ri, nrm));
+        }
+        wp.store(w, k);
+    }
+    if (norm_partials) {
+        const double s = block_sum(nrm, scratch);
+        if (threadIdx.x == 0) norm_partials[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(RT) k_multi_axpy_odd(uint64_t n, const VecTable tab, int nvec,
+                                                       const int *nvec_dev, const double *coef,
+                                                       Cplx<float> *w, double *norm_partials,
+                                                       const int *gate, const int *gate2) {
     if ((gate && *gate == 0) || (gate2 && *gate2 == 0)) return;
     __shared__ double scratch[RW];
     __shared__ double c[2 * (MAX_KRYLOV + 1)];
@@ -201,15 +371,15 @@ __global__ void __launch_bounds__(RT) k_multi_axpy(uint64_t n, const VecTable ta
     const uint64_t hi = lo + chunk < n ? lo + chunk : n;
     double nrm = 0.0;
     for (uint64_t k = lo + threadIdx.x; k < hi; k += RT) {
-        const Cplx<Real> w0 = w[k];
+        const Cplx<float> w0 = w[k];
         double xr = w0.x, xi = w0.y;
         for (int i = 0; i < nv; i++) {
-            const Cplx<Real> u = static_cast<const Cplx<Real> *>(tab.p[i])[k];
+            const Cplx<float> u = static_cast<const Cplx<float> *>(tab.p[i])[k];
             const double cr = c[2 * i], ci = c[2 * i + 1];
             xr = fma(cr, (double)u.x, fma(-ci, (double)u.y, xr));
             xi = fma(cr, (double)u.y, fma(ci, (double)u.x, xi));
         }
-        const Cplx<Real> r{(Real)xr, (Real)xi};
+        const Cplx<float> r{(float)xr, (float)xi};
         w[k] = r;
         nrm = fma((double)r.x, (double)r.x, fma((double)r.y, (double)r.y, nrm));
     }
@@ -225,11 +395,14 @@ void multi_axpy(int dtype, uint64_t n, const VecTable &tab, int nvec, const int 
     RP_REQUIRE(nvec >= 0 && nvec <= MAX_KRYLOV + 1, -2, "too many vectors");
     const int g = reduce_grid();
     if (dtype == 2)
-        k_multi_axpy<double><<<g, RT, 0, st>>>(n, tab, nvec, nvec_dev, coef, (Cplx<double> *)w,
-                                               norm_partials, gate, gate2);
+        k_multi_axpy<double><<<g, RT, 0, st>>>(n, tab, nvec, nvec_dev, coef, w, norm_partials,
+                                               gate, gate2);
+    else if (n % 2 == 0)
+        k_multi_axpy<float><<<g, RT, 0, st>>>(n / 2, tab, nvec, nvec_dev, coef, w, norm_partials,
+                                              gate, gate2);
     else
-        k_multi_axpy<float><<<g, RT, 0, st>>>(n, tab, nvec, nvec_dev, coef, (Cplx<float> *)w,
-                                              norm_partials, gate, gate2);
+        k_multi_axpy_odd<<<g, RT, 0, st>>>(n, tab, nvec, nvec_dev, coef, (Cplx<float> *)w,
+                                           norm_partials, gate, gate2);
     RP_CUDA(cudaGetLastError());
 }
 
