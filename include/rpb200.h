@@ -53,6 +53,12 @@ typedef struct {
     double alg_bytes_dram; /* (G_w + 1) * 2^len * element size, G_w = distinct
                               x >> (tile_exp + log2 window): the compulsory DRAM
                               bytes when source blocks are served from L2 */
+    double smem_bytes;   /* bytes moved through shared memory per apply: one
+                            element per term (after splitting complex
+                            coefficients) and output element, plus every
+                            staged source tile */
+    int nreads;          /* source-element reads per output element (terms) */
+    int pad;
 } rp_ham_info_t;
 
 /* Statistics of one evolve. */

@@ -1,4 +1,5 @@
 // C ABI of librpb200.so: argument checking, error translation, context.
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -315,6 +316,12 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info) {
         info->kernel = p.cfg.direct ? 0 : (p.rows.ok ? 2 : 1);
         info->window = apply_grid(p);
         info->alg_bytes_dram = p.rows.ok ? p.rows.alg_bytes_dram : p.alg_bytes;
+        const double vbytes = std::ldexp(1.0, p.len) * (p.dtype == RP_C128 ? 16.0 : 8.0);
+        const int nt = p.rows.ok ? p.rows.nterms : p.nterms;
+        const int ng = p.rows.ok ? (int)p.rows.groups.size() : p.ngroups;
+        info->nreads = nt;
+        info->smem_bytes = (double)(nt + ng) * vbytes;
+        info->pad = 0;
         if (p.rows.ok) {
             info->tile_exp = p.rows.B;
             info->ngroups = (int)p.rows.groups.size();

@@ -81,7 +81,21 @@ void workspace_release(KryWorkspace &ws) {
 }
 
 void workspace_ensure(KryWorkspace &ws, int len, int dtype, int krydim) {
-    if (ws.dev && ws.len == len && ws.dtype == dtype && ws.krydim == krydim) return;
+    if (ws.dev && ws.len == len && ws.dtype == dtype) {
+        if (krydim <= ws.krydim) return;
+        // a larger basis for the same state: add vectors, keep the rest
+        const size_t vb = ws.D * esize(dtype);
+        while (ws.krydim < krydim) {
+            void *p = nullptr;
+            if (cudaMalloc(&p, vb) != cudaSuccess) {
+                cudaGetLastError();
+                throw Error{-4, "device out of memory for the Krylov workspace"};
+            }
+            ws.u.push_back(p);
+            ws.krydim++;
+        }
+        return;
+    }
     workspace_release(ws);
     ws.len = len;
     ws.dtype = dtype;
@@ -371,10 +385,7 @@ void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_
 void krylov_arnoldi(const ApplyPlan &plan, KryWorkspace &ws, const void *psi, int m,
                     ArnoldiResult &R, cudaStream_t st) {
     RP_REQUIRE(m >= 2 && m <= MAX_KRYLOV, -2, "m must be in [2, 64]");
-    // a step controller varies m from step to step: keep a larger basis
-    // allocation instead of reallocating it
-    const bool same = ws.dev && ws.len == plan.len && ws.dtype == plan.dtype;
-    workspace_ensure(ws, plan.len, plan.dtype, same ? std::max(ws.krydim, m) : m);
+    workspace_ensure(ws, plan.len, plan.dtype, m);
     const uint64_t D = ws.D;
     const int dtype = plan.dtype;
     R = ArnoldiResult{};

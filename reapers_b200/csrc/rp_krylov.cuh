@@ -54,6 +54,9 @@ struct KryWorkspace {
     void **tab = nullptr;    // device copy of the basis pointer table
 };
 
+// At least krydim + 1 basis vectors for states of 2^len elements of dtype:
+// a workspace for the same state shape is kept and grown, never shrunk
+// (rp_workspace_release frees it).
 void workspace_ensure(KryWorkspace &ws, int len, int dtype, int krydim);
 void workspace_release(KryWorkspace &ws);
 

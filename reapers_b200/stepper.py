@@ -159,14 +159,23 @@ def _round2(x):
 # ---------------------------------------------------------------------------
 # Controllers
 # ---------------------------------------------------------------------------
+STRETCH = (1.25, 1.5, 2.0, 3.0, 4.0, 6.0, 8.0)   # step extensions tried on one basis
+
+
 class PlainController:
-    """Expokit's step-size control with a fixed basis size."""
+    """Expokit's step-size control with a fixed basis size.  With
+    stretch=True every accepted step is also tried at the multiples STRETCH of
+    its size on the same basis (one small-matrix launch, no H.psi) and the
+    largest admissible one is taken."""
 
     name = "plain"
     gamma = 0.9
 
-    def __init__(self, m=30):
+    def __init__(self, m=30, stretch=False):
         self.m = int(m)
+        self.stretch = bool(stretch)
+        if self.stretch:
+            self.name = "plain+stretch"
 
     def start(self, ham, T, tol):
         self.T, self.tol = float(T), float(tol)
@@ -176,7 +185,7 @@ class PlainController:
         tol_u = self.tol / self.T
         self.dt_next = _round2((1.0 / anorm) * (fact * tol_u / (4.0 * anorm)) ** (1.0 / m))
 
-    def propose(self, prev):
+    def propose(self, prev, t_left):
         return self.dt_next, self.m, False
 
     def shrink(self, dt, err, m):
@@ -285,12 +294,17 @@ class Mlp:
             pass
 
 
+SMEM_OVER_HBM = 5.7   # B200: shared-memory bandwidth (128 B/clk/SM) over HBM bandwidth
+
+
 def problem_figures(ham):
-    """A, the cost of one H.psi in vector passes: the plan's effective bytes
-    ((source-tile groups + 1) vector streams) over the bytes of one vector."""
+    """A, the cost of one H.psi in units of one streaming pass over a vector:
+    the larger of its compulsory DRAM bytes and its shared-memory gather
+    bytes scaled by the shared-memory / HBM bandwidth ratio, over the bytes
+    of one vector."""
     info = ham.info()
     vec = float(1 << ham.len) * (8 if ham.dtype == 1 else 16)
-    return max(1.0, info["alg_bytes"] / vec)
+    return max(1.0, info["alg_bytes_dram"] / vec, info["smem_bytes"] / SMEM_OVER_HBM / vec)
 
 
 def features(basis, m_prev, tol_u, A):
@@ -308,18 +322,27 @@ def features(basis, m_prev, tol_u, A):
 
 def step_cost(k, A, rho):
     """Modelled cost of one step with k basis vectors, in vector passes:
-    k H.psi products, the orthogonalisation passes (rho per vector, each
-    reading the basis so far and w, writing w) and the fixed overhead."""
-    return k * A + rho * k * (k + 5) / 2.0 + k + 1 + STEP_OVERHEAD
+    k H.psi products; per basis vector j and orthogonalisation pass (rho per
+    vector) a projection pass over the j + 1 vectors so far (w re-read once
+    per group of 8) and an update pass over them (w read and written); the
+    final combination of k vectors and the fixed overhead."""
+    ortho = 1.125 * k * (k + 1) / 2.0 + k * (k + 5) / 2.0   # sum over j < k
+    return k * A + rho * ortho + k + 1 + STEP_OVERHEAD
 
 
 class LearnedController(PlainController):
-    """MLP-proposed (dt, m), checked by the plain error estimate."""
+    """MLP-proposed (dt, m), checked by the plain error estimate.
+
+    When the proposed step reaches the end of the interval, the basis is cut
+    to the smallest size whose admissible step -- estimated from the previous
+    restart's Hessenberg matrix exactly as the training labels are -- still
+    covers the remaining time."""
 
     name = "learned"
 
-    def __init__(self, model, m_first=30, safety=0.95):
-        super().__init__(m_first)
+    def __init__(self, model, m_first=30, safety=0.95, stretch=True):
+        super().__init__(m_first, stretch)
+        self.name = "learned"
         self.model = model
         self.safety = float(safety)
 
@@ -327,17 +350,30 @@ class LearnedController(PlainController):
         super().start(ham, T, tol)
         self.A = problem_figures(ham)
 
-    def propose(self, prev):
+    def propose(self, prev, t_left):
         if prev is None or prev.m_eff < NFEAT + 1:
             return self.dt_next, self.m, False
-        x, s = features(prev, prev.m_eff, self.tol / self.T, self.A)
+        tol_u = self.tol / self.T
+        x, s = features(prev, prev.m_eff, tol_u, self.A)
         y = self.model.predict(x[None, :])[0]
         m = int(np.clip(round(float(y[1]) * 32.0), M_MIN, M_MAX))
         dt = self.safety * math.exp(float(np.clip(y[0], -12.0, 12.0))) / s
         # growth limit: at most 4x the last accepted step
         dt = min(dt, 4.0 * self.dt_last)
+        if dt >= t_left:
+            m = self._last_step_basis(prev, t_left, m, tol_u)
         self.m = m
         return dt, m, True
+
+    @staticmethod
+    def _last_step_basis(prev, t_left, m, tol_u):
+        for k in range(M_MIN, min(m - 1, prev.m_eff) + 1, 2):
+            beta = abs(prev.H[k, k - 1]) if k < prev.m_eff else prev.beta
+            d = admissible_dt(prev.H[None, :k, :k], np.array([beta]), tol_u,
+                              np.array([t_left * 1e-3]), np.array([t_left]))
+            if d[0] >= t_left:
+                return k
+        return m
 
     def accepted(self, basis, dt, err, t_left):
         super().accepted(basis, dt, err, t_left)
@@ -359,7 +395,7 @@ def step_evolve(ham, psi, T, tol=1e-8, controller=None, record=False, max_steps=
     t = 0.0
     prev = None
     st = {"controller": ctl.name, "steps": 0, "applies": 0, "proposals": 0,
-          "proposals_accepted": 0, "rejections": 0, "err_sum": 0.0, "cost": 0.0,
+          "proposals_accepted": 0, "rejections": 0, "stretched": 0, "err_sum": 0.0, "cost": 0.0,
           "ms_mlp": 0.0, "trace": [] if record else None}
     A = problem_figures(ham)
     torch.cuda.synchronize()
@@ -369,7 +405,7 @@ def step_evolve(ham, psi, T, tol=1e-8, controller=None, record=False, max_steps=
             raise RuntimeError("step_evolve: too many steps")
         t_left = T - t
         tm = time.perf_counter()
-        dt, m, learned = ctl.propose(prev)
+        dt, m, learned = ctl.propose(prev, t_left)
         st["ms_mlp"] += (time.perf_counter() - tm) * 1e3 if learned else 0.0
         basis = arnoldi(ham, psi, m)
         st["applies"] += basis.m_eff
@@ -391,6 +427,15 @@ def step_evolve(ham, psi, T, tol=1e-8, controller=None, record=False, max_steps=
             coef, err = step_errors(basis, [dt])
             err = float(err[0])
             ok = err <= tol_u * dt
+        if ctl.stretch and dt < t_left:
+            cands = sorted({min(dt * f, t_left) for f in STRETCH} - {dt})
+            c2, e2 = step_errors(basis, cands)
+            good = [i for i in range(len(cands)) if e2[i] <= tol_u * cands[i]]
+            if good:
+                i = good[-1]
+                dt, err = cands[i], float(e2[i])
+                coef = c2[i:i + 1]
+                st["stretched"] += 1
         combine(basis.beta0 * coef[0], psi)
         if record:
             st["trace"].append({"t": t, "dt": dt, "m": basis.m_eff, "err": err,
