@@ -1,0 +1,157 @@
+// dropin_driver.cc -- the reference library's own host code (State, Krylov,
+// SYK, FermionOpNonBlockForm; its headers compiled unmodified from the
+// reference checkout with REAPERS_NOGPU against eigen_shim/) run twice in one
+// process: on its CPU backend (CPUImpl) and on B200Impl
+// (include/rpb200_impl.hpp, i.e. librpb200's sm_100a kernels).
+//
+// TEST INFRASTRUCTURE ONLY: it shows that B200Impl is a drop-in backend for
+// the reference's unchanged algorithms and measures the difference of every
+// result against the CPU backend.  Built by oracle/Makefile into
+// oracle/_ref/dropin_driver; run by tests/test_gpu_dropin.py.
+//
+// usage: dropin_driver N sparsity seed t krydim
+// prints one JSON object of relative differences (GPU backend vs CPU backend).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <string>
+
+#define REAPERS_NOGPU
+
+#include <reapers.h>
+
+#include "rpb200_impl.hpp"
+
+using namespace REAPERS;
+using namespace REAPERS::Model;
+using namespace REAPERS::EvolutionAlgorithm;
+
+using CSt = State<double, CPUImpl>;
+using GSt = State<double, B200Impl>;
+
+// ||a - b|| / ||b|| with a moved to the host backend
+static double rel_diff(const GSt &g, const CSt &c) {
+    CSt gh(g);
+    double num = 0, den = 0;
+    for (size_t i = 0; i < c.dim(); i++) {
+        auto d = gh[i] - c[i];
+        num += std::norm(std::complex<double>(d.real(), d.imag()));
+        auto v = c[i];
+        den += std::norm(std::complex<double>(v.real(), v.imag()));
+    }
+    return std::sqrt(num / den);
+}
+
+template <typename Ops>
+static double term_diff(const Ops &a, const HostSumOps<double> &b) {
+    if (a.size() != b.size()) return 1e300;
+    double d = 0;
+    auto ib = b.begin();
+    for (auto ia = a.begin(); ia != a.end(); ++ia, ++ib) {
+        if (ia->get_bit_string() != ib->get_bit_string()) return 1e300;
+        d = std::max(d, (double)std::abs(ia->coefficient() - ib->coefficient()));
+    }
+    return d;
+}
+
+int main(int argc, char **argv) {
+    if (argc < 6) {
+        std::fprintf(stderr, "usage: dropin_driver N sparsity seed t krydim\n");
+        return 1;
+    }
+    const int N = std::atoi(argv[1]);
+    const double sp = std::atof(argv[2]);
+    const unsigned seed = (unsigned)std::strtoul(argv[3], nullptr, 10);
+    const double t = std::atof(argv[4]);
+    const int krydim = std::atoi(argv[5]);
+    const int L = N / 2;
+    const double tol = 1e-14;
+
+    // the same model and generator on both backends (inc/syk.h:239-263)
+    SYK<double, CPUImpl, FermionOpNonBlockForm> syk_c(N, sp, 1.0);
+    SYK<double, B200Impl, FermionOpNonBlockForm> syk_g(N, sp, 1.0);
+    std::mt19937 rg_c(seed), rg_g(seed);
+    HostSumOps<double> ham_c = syk_c.gen_ham(rg_c);
+    B200SumOps<double> ham_g = syk_g.gen_ham(rg_g);
+    const double terms = term_diff(ham_g, ham_c);
+
+    // one random state, moved to the device by State's conversion constructor
+    CSt c0(L);
+    {
+        std::mt19937 rs(seed + 1);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        for (size_t i = 0; i < c0.dim(); i++) c0[i] = complex<double>(nd(rs), nd(rs));
+        c0 *= 1.0 / c0.norm();
+    }
+    GSt g0(c0);
+    const double roundtrip = rel_diff(g0, c0);
+    // element access through the device proxy
+    complex<double> e3 = g0[3];
+    const double elem = std::abs(e3 - c0[3]);
+
+    // H psi: State operator* (inc/state.h:335-343)
+    CSt c1 = ham_c * c0;
+    GSt g1 = ham_g * g0;
+    const double apply = rel_diff(g1, c1);
+
+    // the reference's own restarted Krylov (inc/algo.h:267-365) on both backends
+    CSt c2(c0);
+    GSt g2(g0);
+    c2.evolve(ham_c, t, 0.0, krydim, tol);
+    g2.evolve(ham_g, t, 0.0, krydim, tol);
+    const double evolve = rel_diff(g2, c2);
+
+    // the GPU-resident Krylov through the same State call
+    GSt g3(g0);
+    g3.evolve<B200Krylov>(ham_g, t, 0.0, krydim, tol);
+    const double evolve_fused = rel_diff(g3, c2);
+
+    // imaginary time as well: exp(-(beta + i t) H)
+    CSt c4(c0);
+    GSt g4(g0);
+    c4.evolve(ham_c, 0.3 * t, 0.2, krydim, tol);
+    g4.evolve<B200Krylov>(ham_g, 0.3 * t, 0.2, krydim, tol);
+    const double evolve_beta = rel_diff(g4, c4);
+
+    // OTOC sequence of examples/simple-syk-krylov.cc:42-57 with W = b_{N-1}, V = b_{N-2}
+    HostSumOps<double> Wc(syk_c.fermion_ops(N - 1)), Vc(syk_c.fermion_ops(N - 2));
+    B200SumOps<double> Wg(syk_g.fermion_ops(N - 1)), Vg(syk_g.fermion_ops(N - 2));
+    CSt pc(c0);
+    GSt pg(g0);
+    pc *= Vc;
+    pg *= Vg;
+    pc.evolve(ham_c, t, 0.0, krydim, tol);
+    pg.evolve<B200Krylov>(ham_g, t, 0.0, krydim, tol);
+    pc *= Wc;
+    pg *= Wg;
+    pc.evolve(ham_c, -t, 0.0, krydim, tol);
+    pg.evolve<B200Krylov>(ham_g, -t, 0.0, krydim, tol);
+    pc *= Vc;
+    pg *= Vg;
+    pc.evolve(ham_c, t, 0.0, krydim, tol);
+    pg.evolve<B200Krylov>(ham_g, t, 0.0, krydim, tol);
+    pc *= Wc;
+    pg *= Wg;
+    pc.evolve(ham_c, -t, 0.0, krydim, tol);
+    pg.evolve<B200Krylov>(ham_g, -t, 0.0, krydim, tol);
+    const auto Fc = c0 * pc;
+    const auto Fg = g0 * pg;
+    const double otoc = std::abs(Fg - Fc) / std::abs(c0 * c0);
+
+    // changing the operator drops its device table (release()); the next
+    // apply uploads the new term list
+    ham_c += SpinOp<double>::sigma_x(0) * SpinOp<double>::sigma_y(1);
+    ham_g += SpinOp<double>::sigma_x(0) * SpinOp<double>::sigma_y(1);
+    CSt c5 = ham_c * c0;
+    GSt g5 = ham_g * g0;
+    const double mutate = rel_diff(g5, c5);
+
+    std::printf(
+        "{\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
+        "\"apply\": %.3e, \"evolve_ref_krylov\": %.3e, \"evolve_b200krylov\": %.3e, "
+        "\"evolve_beta\": %.3e, \"otoc\": %.3e, \"F\": [%.12e, %.12e], \"mutate\": %.3e}\n",
+        N, ham_c.size(), terms, roundtrip, elem, apply, evolve, evolve_fused, evolve_beta, otoc,
+        (double)Fc.real(), (double)Fc.imag(), mutate);
+    return 0;
+}

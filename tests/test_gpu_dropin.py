@@ -1,0 +1,45 @@
+"""The reference's own host code on B200Impl (include/rpb200_impl.hpp).
+
+oracle/_ref/dropin_driver instantiates the reference's State, Krylov, SYK and
+FermionOpNonBlockForm templates twice in one process -- on the reference's
+CPUImpl and on B200Impl, which routes every backend call through the C ABI
+to the sm_100a kernels -- and reports the relative difference of each result:
+the SYK term list, the host->device->host state round trip, element access,
+State operator* (H.psi), the reference's restarted Krylov evolve, the
+GPU-resident Krylov selected as State::evolve<B200Krylov>, imaginary-time
+evolution, the OTOC sequence of examples/simple-syk-krylov.cc, and an apply
+after the operator is changed (device table dropped and rebuilt).
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "dropin_driver")
+
+
+def test_dropin_driver_is_built_against_librpb200():
+    assert os.path.exists(DRIVER), "oracle/_ref/dropin_driver was not built"
+    out = subprocess.run(["ldd", DRIVER], capture_output=True, text=True).stdout
+    line = [ln for ln in out.splitlines() if "librpb200" in ln]
+    assert line and "not found" not in line[0], out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,sp,seed,t,krydim", [
+    (16, 0.0, 3, 1.0, 8),      # dense SYK, 1820 terms >= 2^8: the reference takes its dense path
+    (20, 8.0, 5, 2.0, 10),     # sparse SYK k = 8
+    (24, 8.0, 7, 1.5, 12),     # sparse SYK, 12 qubits
+])
+def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
+    r = subprocess.run([DRIVER, str(N), str(sp), str(seed), str(t), str(krydim)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["term_diff"] == 0.0
+    assert d["roundtrip"] == 0.0 and d["elem"] == 0.0
+    for k in ("apply", "evolve_ref_krylov", "evolve_b200krylov", "evolve_beta", "mutate"):
+        assert d[k] <= 1e-12, (k, d)
+    assert d["otoc"] <= 1e-11, d
