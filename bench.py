@@ -223,7 +223,8 @@ def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40)
     out = {"workload": f"{nreal} sparse-SYK realisations (k=8, N cycling {list(sizes)}) x "
                        f"{nstates} states = {len(problems)} problems, t in "
                        f"{[float(round(t, 4)) for t in times]} of 40 points on [0, 20], m={krydim}",
-           "tiles": {k: v["tile"] for k, v in tuned.items()}, "per_size": {}}
+           "tiles": {k: v["tile"] for k, v in tuned.items()},
+           "teams": {k: v["team"] for k, v in tuned.items()}, "per_size": {}}
     tot_batch = tot_seq = tot_best = 0.0
     err = 0.0
     for N in sizes:

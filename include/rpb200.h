@@ -197,7 +197,7 @@ int rp_mlp_destroy(rp_mlp_t net);
 
 /* --- batched OTOC (the outer loops of examples/syk.cc:417-475 and
  * examples/simple-syk-krylov.cc:42-57 over many disorder realisations and
- * states, run as one persistent launch per time step) ---------------------- */
+ * states, run as one persistent launch per time step and team size) ------- */
 typedef struct rp_batch *rp_batch_t;
 /* nprob problems; problem p has len[p] qubits (8..30), nterms[p] terms
  * (bits[p], coeff[p] as for rp_ham_create), W and V single Pauli strings
@@ -211,14 +211,23 @@ int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nte
                     const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
                     const double *vcoeff, const void *const *psi0, const int *tile, int krydim,
                     double tol, int max_restarts);
+/* As rp_batch_create, with team[p] the number of CTAs (a thread-block
+ * cluster: 1, 2, 4, 8 or 16; 0 = the default for the qubit count) that share
+ * problem p; problems of one team size form one launch per time step.  team
+ * may be NULL. */
+int rp_batch_create_ex(rp_batch_t *b, int nprob, const int *len, const int64_t *nterms,
+                       const uint64_t *const *bits, const double *const *coeff,
+                       const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
+                       const double *vcoeff, const void *const *psi0, const int *tile,
+                       const int *team, int krydim, double tol, int max_restarts);
 /* F[(p * ntimes + k) * 2 + {0,1}] = <psi0| W(t_k) V W(t_k) V |psi0> of problem
  * p (beta = 0), applies[p * ntimes + k] its H.psi count (either may be NULL).
- * One persistent launch per time step; with use_graph the launches are
- * captured once into a CUDA graph and replayed. */
+ * One persistent launch per time step and team size; with use_graph the
+ * launches are captured once into a CUDA graph and replayed. */
 int rp_batch_otoc(rp_batch_t b, int ntimes, const double *times, double *F, int *applies,
                   int use_graph);
-/* One persistent launch doing only napplies H.psi products per problem (no
- * Krylov); *ms = its device time.  Used by the tile autotuner. */
+/* One persistent launch (per team size) doing only napplies H.psi products
+ * per problem (no Krylov); *ms = the device time.  Used by the autotuner. */
 int rp_batch_probe(rp_batch_t b, int napplies, double *ms);
 int rp_batch_destroy(rp_batch_t b);
 

@@ -182,8 +182,9 @@ class BatchOTOC:
     qubit counts) run by one persistent launch per time step (rp_batch_*).
 
     problems: list of dicts with keys len, bits, coeff, w (bits, coeff),
-    v (bits, coeff), psi0 (complex64 CUDA tensor) and optionally tile (8..11).
-    FP32 vectors, FP64 Krylov internals (the mixed-precision form)."""
+    v (bits, coeff), psi0 (complex64 CUDA tensor) and optionally tile (8..11)
+    and team (CTAs per problem: 1, 2, 4, 8 or 16).  FP32 vectors, FP64 Krylov
+    internals (the mixed-precision form)."""
 
     def __init__(self, problems, krydim=16, tol=1.2e-7, max_restarts=16):
         n = len(problems)
@@ -211,9 +212,10 @@ class BatchOTOC:
                 raise ValueError("batched states are complex64")
         psis = (C.c_void_p * n)(*[p["psi0"].data_ptr() for p in problems])
         tiles = (C.c_int * n)(*[int(p.get("tile", 0)) for p in problems])
+        teams = (C.c_int * n)(*[int(p.get("team", 0)) for p in problems])
         h = C.c_void_p()
-        _lib.call("rp_batch_create", C.byref(h), n, lens, nterms, bitp, coefp, wb, wc, vb, vc,
-                  psis, tiles, int(krydim), float(tol), int(max_restarts))
+        _lib.call("rp_batch_create_ex", C.byref(h), n, lens, nterms, bitp, coefp, wb, wc, vb, vc,
+                  psis, tiles, teams, int(krydim), float(tol), int(max_restarts))
         self._h = h
         self.n = n
 

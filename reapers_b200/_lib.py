@@ -97,6 +97,12 @@ _SIGS = {
                                   C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_double), C.POINTER(_VP), C.POINTER(C.c_int),
                                   C.c_int, C.c_double, C.c_int]),
+    "rp_batch_create_ex": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_uint64)),
+                                     C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_double), C.POINTER(_VP), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.c_int, C.c_double, C.c_int]),
     "rp_batch_otoc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int), C.c_int]),
     "rp_batch_probe": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),

@@ -1,15 +1,15 @@
-"""Autotuner for the batched OTOC kernel's tile exponent.
+"""Autotuner for the batched OTOC kernel's tile exponent and team size.
 
-For every distinct (qubit count, number of source-tile groups per tile
-exponent, precision, Krylov dimension) in a batch, the tuner times one
-persistent launch doing two H.psi products per problem (rp_batch_probe) on a
-sample of the batch's own problems of that size (up to one per SM, so the
-memory system is loaded as in the real run), for each tile exponent B in
-8..min(11, L), and keeps the fastest.  Results are
-cached in a JSON file (``RPB200_TUNE_CACHE`` or
-``~/.cache/reapers_b200/tune.json``) keyed by
-``L{len}-G{groups at B=11, to the nearest 32}-c64-m{krydim}``, so later batches of the same
-shape skip the search.
+For every distinct (qubit count, number of source-tile groups, precision,
+Krylov dimension) in a batch, the tuner times one persistent launch doing
+two H.psi products per problem (rp_batch_probe) on a sample of the batch's
+own problems of that size (up to one per SM, so the memory system is loaded
+as in the real run), for each tile exponent B in 8..min(11, L) and each
+team size (CTAs per problem, a thread-block cluster) C in 1, 2, 4, 8, 16
+with C <= 2^(L-B) tiles, and keeps the fastest pair.  Results are cached in
+a JSON file (``RPB200_TUNE_CACHE`` or ``~/.cache/reapers_b200/tune.json``)
+keyed by ``L{len}-G{groups at B=11, to the nearest 32}-c64-m{krydim}-t``, so
+later batches of the same shape skip the search.
 """
 from __future__ import annotations
 
@@ -50,12 +50,12 @@ def shape_key(prob, krydim):
     32 share a tuning (disorder realisations of one model differ slightly)."""
     L = int(prob["len"])
     g = len(np.unique(S.xmask(prob["bits"]) >> np.uint64(min(11, L))))
-    return f"L{L}-G{32 * round(g / 32)}-c64-m{krydim}"
+    return f"L{L}-G{32 * round(g / 32)}-c64-m{krydim}-t"
 
 
 def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, sample=None,
          force=False, log=None):
-    """Set problems[i]['tile'] to the tuned exponent; returns {key: record}."""
+    """Set problems[i]['tile'] and ['team'] to the tuned pair; returns {key: record}."""
     import torch
     from . import BatchOTOC
     cache = {} if force else _load()
@@ -65,25 +65,28 @@ def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, sample=None,
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     out = {}
     for key, idx in by_key.items():
-        if key in cache:
-            best = cache[key]["tile"]
-        else:
+        if key not in cache:
             L = int(problems[idx[0]]["len"])
             n = sample or min(len(idx), sms)
-            cand = list(range(8, min(11, L) + 1))
             timings = {}
-            for B in cand:
-                probs = [dict(problems[j], tile=B) for j in idx[:n]]
-                b = BatchOTOC(probs, krydim=krydim, tol=tol, max_restarts=max_restarts)
-                b.probe(1)                                   # warm-up
-                timings[B] = b.probe(2) / 1e3                # two H.psi per problem
-                b.close()
+            for B in range(8, min(11, L) + 1):
+                for C in (1, 2, 4, 8, 16):
+                    if C > (1 << (L - B)):
+                        continue
+                    probs = [dict(problems[j], tile=B, team=C) for j in idx[:n]]
+                    b = BatchOTOC(probs, krydim=krydim, tol=tol, max_restarts=max_restarts)
+                    b.probe(1)                                   # warm-up
+                    timings[f"B{B}-C{C}"] = b.probe(2) / 1e3     # two H.psi per problem
+                    b.close()
             best = min(timings, key=timings.get)
-            cache[key] = {"tile": best, "seconds": timings, "sample": n, "probe": "2 H.psi"}
+            B, C = (int(v[1:]) for v in best.split("-"))
+            cache[key] = {"tile": B, "team": C, "seconds": timings, "sample": n,
+                          "probe": "2 H.psi"}
             if log:
-                log(f"autotune {key}: {timings} -> B={best}")
+                log(f"autotune {key}: {timings} -> {best}")
         for j in idx:
-            problems[j]["tile"] = int(best)
+            problems[j]["tile"] = int(cache[key]["tile"])
+            problems[j]["team"] = int(cache[key]["team"])
         out[key] = cache[key]
     _save(cache)
     return out

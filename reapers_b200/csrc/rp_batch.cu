@@ -1,23 +1,37 @@
-// Batched OTOC on one GPU: one persistent launch per time step.
+// Batched OTOC on one GPU: one persistent launch per time step and team size.
 //
 // Work item = one problem (a disorder realisation x random state, any qubit
-// count).  A CTA takes items from an atomic queue and runs the whole OTOC
-// point for its item alone, in the operator order of
+// count).  A team -- a thread-block cluster of C CTAs (C = 1..16, chosen per
+// problem size) -- takes items from an atomic queue and runs the whole OTOC
+// point for its item, in the operator order of
 // examples/simple-syk-krylov.cc:42-57 at beta = 0:
 //     psi = V psi0; e^{-iHt}; W; e^{iHt}; V; e^{-iHt}; W; e^{iHt}; <psi0|psi>,
 // each evolve being the reference's restarted Krylov (inc/algo.h:77-173,
 // 267-365: same pass criterion, breakdown rule, Hfull growth and ||Hexp0||
-// test) executed by the CTA: H.psi through a 4-stage bulk-copy ring of
-// 2^B-element source tiles in shared memory (tile exponent B per problem,
-// chosen by the autotuner), projections and updates as CTA-wide passes with
-// FP64 accumulation, FP64 H / Hfull / Pade-13 exponential in per-CTA global
-// scratch.  Problems are independent, so CTAs never wait on one another.
-// Vectors are FP32 (the mixed-precision form); everything else FP64.
+// test).  The team splits every vector pass: CTA r owns elements
+// [r n / C, (r + 1) n / C) of copies, Pauli strings, projections and
+// updates, and output tiles r, r + C, ... of H.psi, so the team's tiles in
+// flight form a window of C consecutive tiles whose shared source tiles
+// come from L2.  H.psi streams 2^B-element source tiles through a 4-stage
+// bulk-copy ring per CTA (B per problem, chosen by the autotuner), whose
+// source reads carry an L2 evict-last hint.
+// Reductions: every CTA publishes its partial sums (and an ok flag) in
+// shared memory, the cluster barrier (release/acquire at cluster scope)
+// separates phases, and every CTA adds the C partials in rank order through
+// distributed shared memory -- so all CTAs hold bit-identical sums and take
+// identical control decisions.  The small FP64 work (H, Hfull, Pade-13 exp)
+// is done by CTA 0 and its coefficients read by the others the same way.
+// Teams never wait on other teams.  Vectors are FP32 (the mixed-precision
+// form); everything else FP64.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstring>
 
 #include "rp_batch.cuh"
 #include "rp_expm_impl.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace rp {
 
@@ -27,8 +41,8 @@ constexpr int BST = 4;           // shared-memory stages of the H.psi ring
 constexpr int BMAXK = 32;        // largest krydim of the batched form
 
 struct BatchArgs {
-    const BatchProblem *probs;
-    int nprob, krydim, max_restarts, ti, ntimes, hcap;
+    const BatchProblem *probs;   // this launch's problems (one team size)
+    int nprob, out_base, krydim, max_restarts, ti, ntimes, hcap;
     int probe;          // > 0: only `probe` H.psi products per item (tuning)
     double t, tol;
     double *F;
@@ -41,19 +55,31 @@ struct BatchArgs {
 
 struct BatchShared {
     double red[2 * BNW];
+    double part[2][4];            // published partials: [buffer][re, im, ok, -]
     double sigma[BMAXK + 1];
     double hacc[2 * (BMAXK + 1)];
     double coef[2 * (BMAXK + 1)];
     double nrm;
     Cplx<float> *u[BMAXK + 1];
     int item;
+    int pbuf;                     // which part[] buffer the next reduction uses
 };
 
 __device__ __forceinline__ void proxy_fence_global() {
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
-// Fixed-order sums over the CTA, broadcast to every thread.
+// The team of one problem: cluster rank and size, and this CTA's share of
+// an n-element pass.
+struct Team {
+    unsigned rank, size;
+    __device__ uint32_t lo(uint32_t n) const { return (uint32_t)(((uint64_t)n * rank) / size); }
+    __device__ uint32_t hi(uint32_t n) const { return (uint32_t)(((uint64_t)n * (rank + 1)) / size); }
+};
+
+__device__ __forceinline__ void team_sync() { cg::this_cluster().sync(); }
+
+// Fixed-order sums over the CTA, broadcast to every thread of the CTA.
 __device__ __forceinline__ void cta_sum2(double &a, double &b, double *red) {
     a = warp_sum(a);
     b = warp_sum(b);
@@ -72,50 +98,87 @@ __device__ __forceinline__ void cta_sum2(double &a, double &b, double *red) {
     b = cb.value();
 }
 
+// Team-wide fixed-order sums of (a, b) and AND of ok, identical in every
+// CTA.  One cluster barrier; the two partial buffers alternate, so a buffer
+// is rewritten only after every CTA has passed the barrier that follows its
+// reads.
+__device__ bool team_reduce(const Team &tm, double &a, double &b, bool ok, BatchShared &S) {
+    cta_sum2(a, b, S.red);
+    const int buf = S.pbuf;
+    if (threadIdx.x == 0) {
+        S.part[buf][0] = a;
+        S.part[buf][1] = b;
+        S.part[buf][2] = ok ? 1.0 : 0.0;
+    }
+    team_sync();
+    cg::cluster_group cl = cg::this_cluster();
+    CompSum ca, cb;
+    bool all = true;
+    for (unsigned r = 0; r < tm.size; r++) {
+        const double *pr = cl.map_shared_rank(&S.part[buf][0], r);
+        ca.add(pr[0]);
+        cb.add(pr[1]);
+        all = all && pr[2] != 0.0;
+    }
+    a = ca.value();
+    b = cb.value();
+    __syncthreads();
+    if (threadIdx.x == 0) S.pbuf = buf ^ 1;
+    __syncthreads();
+    return all;
+}
+
+__device__ __forceinline__ bool team_and(const Team &tm, bool ok, BatchShared &S) {
+    double a = 0.0, b = 0.0;
+    return team_reduce(tm, a, b, ok, S);
+}
+
 // <a|b> over n elements.
-__device__ void cta_dot(const Cplx<float> *a, const Cplx<float> *b, uint32_t n, double *red,
-                        double &re, double &im) {
+__device__ void team_dot(const Team &tm, const Cplx<float> *a, const Cplx<float> *b, uint32_t n,
+                         BatchShared &S, double &re, double &im) {
     double sr = 0.0, si = 0.0;
-    for (uint32_t k = threadIdx.x; k < n; k += BT) {
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
         const Cplx<float> x = a[k], y = b[k];
         sr = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, sr));
         si = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, si));
     }
-    cta_sum2(sr, si, red);
+    team_reduce(tm, sr, si, true, S);
     re = sr;
     im = si;
 }
 
-__device__ void cta_copy(Cplx<float> *dst, const Cplx<float> *src, uint32_t n) {
-    for (uint32_t k = threadIdx.x; k < n; k += BT) dst[k] = src[k];
+// Element passes end with the generic-proxy writes fenced for the bulk
+// copies of later H.psi products, and a team barrier.
+__device__ void team_copy(const Team &tm, Cplx<float> *dst, const Cplx<float> *src, uint32_t n) {
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) dst[k] = src[k];
     proxy_fence_global();
-    __syncthreads();
+    team_sync();
 }
 
-__device__ void cta_zero(Cplx<float> *dst, uint32_t n) {
-    for (uint32_t k = threadIdx.x; k < n; k += BT) dst[k] = Cplx<float>{0.f, 0.f};
+__device__ void team_zero(const Team &tm, Cplx<float> *dst, uint32_t n) {
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) dst[k] = Cplx<float>{0.f, 0.f};
     proxy_fence_global();
-    __syncthreads();
+    team_sync();
 }
 
 // out[k] = c (-1)^popc(z & (k ^ x)) in[k ^ x]  (SpinOp::apply, inc/ops.h:421-440)
-__device__ void cta_string(uint32_t x, uint32_t z, float cr, float ci, const Cplx<float> *in,
-                           Cplx<float> *out, uint32_t n) {
-    for (uint32_t k = threadIdx.x; k < n; k += BT) {
+__device__ void team_string(const Team &tm, uint32_t x, uint32_t z, float cr, float ci,
+                            const Cplx<float> *in, Cplx<float> *out, uint32_t n) {
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
         const uint32_t m = k ^ x;
         const float s = (__popc(z & m) & 1) ? -1.f : 1.f;
         const Cplx<float> v = in[m];
         out[k] = Cplx<float>{s * (cr * v.x - ci * v.y), s * (cr * v.y + ci * v.x)};
     }
     proxy_fence_global();
-    __syncthreads();
+    team_sync();
 }
 
-// w += sum_{i < nv} coef_i u_i, returning ||w||^2 when want_norm.
-__device__ double cta_axpy(Cplx<float> *const *u, const double *coef, int nv, Cplx<float> *w,
-                           uint32_t n, double *red, bool want_norm) {
+// w += sum_{i < nv} coef_i u_i over the team; returns ||w||^2 (team-wide).
+__device__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double *coef, int nv,
+                            Cplx<float> *w, uint32_t n, BatchShared &S) {
     double nrm = 0.0;
-    for (uint32_t k = threadIdx.x; k < n; k += BT) {
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
         const Cplx<float> w0 = w[k];
         double xr = w0.x, xi = w0.y;
         for (int i = 0; i < nv; i++) {
@@ -130,51 +193,53 @@ __device__ double cta_axpy(Cplx<float> *const *u, const double *coef, int nv, Cp
     }
     proxy_fence_global();
     double dummy = 0.0;
-    if (want_norm) {
-        cta_sum2(nrm, dummy, red);
-    } else {
-        __syncthreads();
-    }
+    team_reduce(tm, nrm, dummy, true, S);
     return nrm;
 }
 
-// out = scale * H in, source tiles streamed through the shared-memory ring.
-// git counts ring items across calls (stage = git % BST, parity (git/BST)&1).
+// out = scale * H in over the team's output tiles (rank, rank + C, ...),
+// source tiles streamed through this CTA's shared-memory ring.  git counts
+// ring items across calls (stage = git % BST, parity (git/BST)&1).  Returns
+// false in every CTA of the team if a bounded wait gave up in any of them.
 template <int B>
-__device__ bool cta_apply(const BatchProblem &P, const Cplx<float> *in, Cplx<float> *out,
-                          double scale, unsigned char *stages, uint64_t *full, long &git,
-                          unsigned *err) {
+__device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, const Cplx<float> *in,
+                           Cplx<float> *out, double scale, unsigned char *stages, uint64_t *full,
+                           long &git, BatchShared &S, unsigned *err) {
     constexpr int TILE = 1 << B, E = TILE / BT;
     constexpr unsigned TB = TILE * sizeof(Cplx<float>);
-    const long total = (long)P.ntiles * P.ngroups;
+    const int my_tiles = P.ntiles > (int)tm.rank ? (P.ntiles - 1 - (int)tm.rank) / (int)tm.size + 1 : 0;
+    const long total = (long)my_tiles * P.ngroups;
     const uint32_t t = threadIdx.x;
+    const uint64_t keep = l2_policy_evict_last();   // the input is re-read once per group
     auto issue = [&](long i) {
         const long gi = git + i;
         const int s = (int)(gi % BST);
-        const int o = (int)(i / P.ngroups), g = (int)(i % P.ngroups);
+        const int o = (int)tm.rank + (int)(i / P.ngroups) * (int)tm.size, g = (int)(i % P.ngroups);
         const uint32_t src = (uint32_t)o ^ P.groups[g].xh;
         mbar_arrive_expect_tx(&full[s], TB);
-        bulk_g2s(stages + (size_t)s * TB, in + ((size_t)src << B), TB, &full[s]);
+        bulk_g2s_hint(stages + (size_t)s * TB, in + ((size_t)src << B), TB, &full[s], keep);
     };
     if (t == 0) {
         proxy_fence_global();
         for (long i = 0; i < BST - 1 && i < total; i++) issue(i);
     }
+    bool ok = true;
     float ar[E], ai[E];
     for (long it = 0; it < total; ++it) {
         const long gi = git + it;
         const int s = (int)(gi % BST);
         const unsigned par = (unsigned)((gi / BST) & 1);
-        const int o = (int)(it / P.ngroups), g = (int)(it % P.ngroups);
+        const int o = (int)tm.rank + (int)(it / P.ngroups) * (int)tm.size;
+        const int g = (int)(it % P.ngroups);
         const bool okw = mbar_wait_bounded(&full[s], par, err);
         if (!__syncthreads_and(okw)) {
-            // drain the copies still in flight, then give up
+            // drain the copies still in flight, then stop this CTA's share
             if (t == 0)
                 for (long i = it; i < it + BST - 1 && i < total; i++)
                     mbar_wait_bounded(&full[(git + i) % BST], (unsigned)(((git + i) / BST) & 1), err);
             __syncthreads();
-            git += total;
-            return false;
+            ok = false;
+            break;
         }
         // every thread is past this item's barrier, so the stage of item it-1
         // is free: prefetch item it + BST - 1 into it
@@ -222,19 +287,20 @@ __device__ bool cta_apply(const BatchProblem &P, const Cplx<float> *in, Cplx<flo
     }
     git += total;
     proxy_fence_global();
-    __syncthreads();
-    return true;
+    return team_and(tm, ok, S);
 }
 
-// psi <- exp(-i t H) psi by the reference's restarted Krylov, run by one CTA.
+// psi <- exp(-i t H) psi by the reference's restarted Krylov, run by a team.
 template <int B>
-__device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_real,
-                           const BatchArgs &a, char *slot, BatchShared &S, unsigned char *stages,
-                           uint64_t *full, double *esmem, long &git, int &applies) {
+__device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *psi,
+                            double t_real, const BatchArgs &a, char *slot, BatchShared &S,
+                            unsigned char *stages, uint64_t *full, double *esmem, long &git,
+                            int &applies) {
     if (t_real == 0.0) return true;   // State::evolve returns at t = beta = 0
     const uint32_t n = 1u << P.len;
     const int m = a.krydim;
     const double eta = 1.0 / sqrt(2.0);
+    const bool lead = tm.rank == 0;
     Cplx<float> *y = reinterpret_cast<Cplx<float> *>(slot + (size_t)(m + 1) * a.vec_stride);
     cd *H = reinterpret_cast<cd *>(slot + (size_t)(m + 4) * a.vec_stride);
     cd *hfull = H + m * m;
@@ -244,27 +310,33 @@ __device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_rea
             S.u[i] = reinterpret_cast<Cplx<float> *>(slot + (size_t)i * a.vec_stride);
     __syncthreads();
     double b2, dummy;
-    cta_dot(psi, psi, n, S.red, b2, dummy);
+    team_dot(tm, psi, psi, n, S, b2, dummy);
     const double beta0 = sqrt(b2);
     if (beta0 == 0.0) return true;
-    cta_copy(S.u[0], psi, n);
-    cta_zero(y, n);
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
+        S.u[0][k] = psi[k];
+        y[k] = Cplx<float>{0.f, 0.f};
+    }
+    proxy_fence_global();
     if (threadIdx.x == 0) S.sigma[0] = 1.0 / beta0;
-    __syncthreads();
+    team_sync();
     double oldbeta = 0.0, beta = 0.0;
     for (int cycle = 1;; cycle++) {
         const int base = (cycle - 1) * m;
         if (base + m > a.hcap) {   // bounded by max_restarts on the host; defensive
-            atomicOr(a.err, DEV_ERR_BOUNDS);
-            return false;
+            if (lead && threadIdx.x == 0) atomicOr(a.err, DEV_ERR_BOUNDS);
+            return false;          // every CTA of the team takes this branch
         }
-        for (int e = threadIdx.x; e < 2 * m * m; e += BT) reinterpret_cast<double *>(H)[e] = 0.0;
+        if (lead) {
+            for (int e = threadIdx.x; e < 2 * m * m; e += BT) reinterpret_cast<double *>(H)[e] = 0.0;
+        }
         __syncthreads();
         int m_eff = m;
         bool brokedown = false;
         for (int j = 0; j < m; j++) {
             Cplx<float> *w = S.u[j + 1];
-            if (!cta_apply<B>(P, S.u[j], w, S.sigma[j], stages, full, git, a.err)) return false;
+            if (!team_apply<B>(tm, P, S.u[j], w, S.sigma[j], stages, full, git, S, a.err))
+                return false;
             applies++;
             double old = 1.0, norm = eta / 2;
             int niter = 0;
@@ -272,7 +344,7 @@ __device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_rea
                 niter++;
                 for (int i = 0; i <= j; i++) {
                     double hr, hi;
-                    cta_dot(S.u[i], w, n, S.red, hr, hi);
+                    team_dot(tm, S.u[i], w, n, S, hr, hi);
                     const double sg = S.sigma[i];
                     hr *= sg;
                     hi *= sg;
@@ -284,12 +356,12 @@ __device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_rea
                     }
                 }
                 __syncthreads();
-                const double nn2 = cta_axpy(S.u, S.coef, j + 1, w, n, S.red, true);
+                const double nn2 = team_axpy(tm, S.u, S.coef, j + 1, w, n, S);
                 old = norm;
                 norm = sqrt(nn2);
             }
             beta = norm;
-            if (threadIdx.x == 0) {
+            if (lead && threadIdx.x == 0) {
                 for (int i = 0; i <= j; i++) H[i + j * m] = cd{S.hacc[2 * i], S.hacc[2 * i + 1]};
             }
             const bool ok = norm != 0.0 && norm >= eta * old;
@@ -300,45 +372,55 @@ __device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_rea
                 break;
             }
             if (threadIdx.x == 0) {
-                if (j != m - 1) H[(j + 1) + j * m] = cd{norm, 0.0};
+                if (lead && j != m - 1) H[(j + 1) + j * m] = cd{norm, 0.0};
                 S.sigma[j + 1] = 1.0 / norm;
             }
             __syncthreads();
         }
-        // Hfull = [OldHfull 0; 0..0 oldbeta H] (inc/algo.h:303-328)
         const int nn = base + m_eff;
-        for (int e = threadIdx.x; e < nn * nn; e += BT) {
-            const int i = e % nn, j = e / nn;
-            if (i >= base || j >= base) hfull[i + (size_t)j * a.hcap] = cd{0.0, 0.0};
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && cycle > 1) hfull[base + (size_t)(base - 1) * a.hcap] = cd{oldbeta, 0.0};
-        for (int e = threadIdx.x; e < m_eff * m_eff; e += BT) {
-            const int i = e % m_eff, j = e / m_eff;
-            hfull[(base + i) + (size_t)(base + j) * a.hcap] = H[i + j * m];
-        }
-        __syncthreads();
-        cd *A = escr, *E = escr + (size_t)nn * nn, *ws = E + (size_t)nn * nn;
-        const cd f{0.0, -t_real};
-        for (int e = threadIdx.x; e < nn * nn; e += BT) {
-            const int i = e % nn, j = e / nn;
-            A[e] = cmul(f, hfull[i + (size_t)j * a.hcap]);
-        }
-        __syncthreads();
-        expm_block(nn, A, E, ws, esmem);
-        if (threadIdx.x == 0) {
-            double sq = 0.0;
-            for (int i = 0; i < m_eff; i++) {
-                const cd e = E[base + i];
-                sq += e.x * e.x + e.y * e.y;
-                const double c = beta0 * S.sigma[i];
-                S.coef[2 * i] = c * e.x;
-                S.coef[2 * i + 1] = c * e.y;
+        if (lead) {
+            // Hfull = [OldHfull 0; 0..0 oldbeta H] (inc/algo.h:303-328)
+            for (int e = threadIdx.x; e < nn * nn; e += BT) {
+                const int i = e % nn, j = e / nn;
+                if (i >= base || j >= base) hfull[i + (size_t)j * a.hcap] = cd{0.0, 0.0};
             }
-            S.nrm = sqrt(sq);
+            __syncthreads();
+            if (threadIdx.x == 0 && cycle > 1) hfull[base + (size_t)(base - 1) * a.hcap] = cd{oldbeta, 0.0};
+            for (int e = threadIdx.x; e < m_eff * m_eff; e += BT) {
+                const int i = e % m_eff, j = e / m_eff;
+                hfull[(base + i) + (size_t)(base + j) * a.hcap] = H[i + j * m];
+            }
+            __syncthreads();
+            cd *A = escr, *E = escr + (size_t)nn * nn, *ws = E + (size_t)nn * nn;
+            const cd f{0.0, -t_real};
+            for (int e = threadIdx.x; e < nn * nn; e += BT) {
+                const int i = e % nn, j = e / nn;
+                A[e] = cmul(f, hfull[i + (size_t)j * a.hcap]);
+            }
+            __syncthreads();
+            expm_block(nn, A, E, ws, esmem);
+            if (threadIdx.x == 0) {
+                double sq = 0.0;
+                for (int i = 0; i < m_eff; i++) {
+                    const cd e = E[base + i];
+                    sq += e.x * e.x + e.y * e.y;
+                    const double c = beta0 * S.sigma[i];
+                    S.coef[2 * i] = c * e.x;
+                    S.coef[2 * i + 1] = c * e.y;
+                }
+                S.nrm = sqrt(sq);
+            }
+        }
+        // the leader's coefficients and convergence norm to the whole team
+        team_sync();
+        if (!lead) {
+            cg::cluster_group cl = cg::this_cluster();
+            const double *lc = cl.map_shared_rank(&S.coef[0], 0);
+            for (int i = threadIdx.x; i < 2 * m_eff; i += BT) S.coef[i] = lc[i];
+            if (threadIdx.x == 0) S.nrm = *cl.map_shared_rank(&S.nrm, 0);
         }
         __syncthreads();
-        cta_axpy(S.u, S.coef, m_eff, y, n, S.red, false);
+        team_axpy(tm, S.u, S.coef, m_eff, y, n, S);   // its barrier also ends the reads above
         const double nrm = S.nrm;
         if ((a.max_restarts && cycle >= a.max_restarts) || brokedown || nrm < a.tol) break;
         // restart from v_m (swap_bufs(0, krydim), inc/algo.h:362)
@@ -351,57 +433,63 @@ __device__ bool cta_evolve(const BatchProblem &P, Cplx<float> *psi, double t_rea
         oldbeta = beta;
         __syncthreads();
     }
-    cta_copy(psi, y, n);
+    team_copy(tm, psi, y, n);
     return true;
 }
 
 template <int B>
-__device__ __noinline__ bool cta_otoc(const BatchProblem &P, const BatchArgs &a, char *slot, BatchShared &S,
-                         unsigned char *stages, uint64_t *full, double *esmem, long &git,
-                         int &applies, double &fr, double &fi) {
+__device__ __noinline__ bool team_otoc(const Team &tm, const BatchProblem &P, const BatchArgs &a,
+                                       char *slot, BatchShared &S, unsigned char *stages,
+                                       uint64_t *full, double *esmem, long &git, int &applies,
+                                       double &fr, double &fi) {
     const uint32_t n = 1u << P.len;
     Cplx<float> *psi = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 2) * a.vec_stride);
     Cplx<float> *tmp = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 3) * a.vec_stride);
     const double t = a.t;
     if (a.probe > 0) {   // tuning: H.psi products only
-        cta_copy(psi, P.psi0, n);
+        team_copy(tm, psi, P.psi0, n);
         for (int r = 0; r < a.probe; r++) {
-            if (!cta_apply<B>(P, (r & 1) ? tmp : psi, (r & 1) ? psi : tmp, 1.0, stages, full, git, a.err))
+            if (!team_apply<B>(tm, P, (r & 1) ? tmp : psi, (r & 1) ? psi : tmp, 1.0, stages, full,
+                               git, S, a.err))
                 return false;
             applies++;
         }
         return true;
     }
-    cta_string(P.vx, P.vz, P.vcr, P.vci, P.psi0, psi, n);
-    if (!cta_evolve<B>(P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
-    cta_string(P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!cta_evolve<B>(P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
-    cta_string(P.vx, P.vz, P.vcr, P.vci, tmp, psi, n);
-    if (!cta_evolve<B>(P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
-    cta_string(P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!cta_evolve<B>(P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
-    cta_dot(P.psi0, tmp, n, S.red, fr, fi);
+    team_string(tm, P.vx, P.vz, P.vcr, P.vci, P.psi0, psi, n);
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    team_string(tm, P.vx, P.vz, P.vcr, P.vci, tmp, psi, n);
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    team_dot(tm, P.psi0, tmp, n, S, fr, fi);
     return true;
 }
 
-__global__ void __launch_bounds__(BT, 1) k_batch_otoc(const BatchArgs a) {
+__global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ BatchShared S;
     __shared__ __align__(8) uint64_t full[BST];
     unsigned char *stages = dsm;
     double *esmem = nullptr;
+    cg::cluster_group cl = cg::this_cluster();
+    const Team tm{cl.block_rank(), cl.num_blocks()};
     if (threadIdx.x == 0) {
         for (int s = 0; s < BST; s++) mbar_init(&full[s], 1);
         fence_barrier_init();
+        S.pbuf = 0;
     }
     __syncthreads();
     long git = 0;
-    char *slot = a.ws + (size_t)blockIdx.x * a.ws_stride;
+    const unsigned team_id = blockIdx.x / tm.size;
+    char *slot = a.ws + (size_t)team_id * a.ws_stride;
     while (true) {
-        if (threadIdx.x == 0) S.item = atomicAdd(&a.counter[a.ti], 1);
-        __syncthreads();
-        const int item = S.item;
-        __syncthreads();
+        if (tm.rank == 0 && threadIdx.x == 0) S.item = atomicAdd(&a.counter[a.ti], 1);
+        team_sync();
+        const int item = *cl.map_shared_rank(&S.item, 0);
+        team_sync();   // the leader rewrites S.item only after everyone read it
         if (item >= a.nprob) break;
         const BatchProblem P = a.probs[item];
         // the expm's factor buffer sits after the largest ring in use
@@ -410,19 +498,22 @@ __global__ void __launch_bounds__(BT, 1) k_batch_otoc(const BatchArgs a) {
         double fr = 0.0, fi = 0.0;
         bool ok = false;
         switch (P.B) {
-            case 8: ok = cta_otoc<8>(P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            case 9: ok = cta_otoc<9>(P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            case 10: ok = cta_otoc<10>(P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            default: ok = cta_otoc<11>(P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
+            case 8: ok = team_otoc<8>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
+            case 9: ok = team_otoc<9>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
+            case 10: ok = team_otoc<10>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
+            default: ok = team_otoc<11>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
         }
-        if (!ok) break;
-        if (threadIdx.x == 0) {
-            a.F[((size_t)item * a.ntimes + a.ti) * 2] = fr;
-            a.F[((size_t)item * a.ntimes + a.ti) * 2 + 1] = fi;
-            a.applies[(size_t)item * a.ntimes + a.ti] = applies;
+        if (!ok) break;   // identical in every CTA of the team
+        if (tm.rank == 0 && threadIdx.x == 0) {
+            const size_t o = (size_t)(a.out_base + item) * a.ntimes + a.ti;
+            a.F[o * 2] = fr;
+            a.F[o * 2 + 1] = fi;
+            a.applies[o] = applies;
         }
         __syncthreads();
     }
+    // no CTA leaves while another may still read its shared memory
+    team_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -453,10 +544,30 @@ static size_t dyn_smem(int maxB, int hcap) {
     return (size_t)BST * ((size_t)1 << maxB) * sizeof(Cplx<float>) + (size_t)(2 * hcap + 64) * sizeof(double);
 }
 
+// Default team size: one CTA up to 2^16 elements, doubling per qubit above,
+// at most 16 (the largest thread-block cluster).
+static int default_team(int len) { return std::min(16, 1 << std::max(0, len - 16)); }
+
+static cudaLaunchConfig_t class_config(const BatchClass &c, size_t smem, cudaStream_t st,
+                                       cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(c.nslots * c.team), 1, 1);
+    cfg.blockDim = dim3(BT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)c.team;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
 void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms,
                  const uint64_t *const *bits, const double *const *coeff, const uint64_t *wbits,
                  const double *wcoeff, const uint64_t *vbits, const double *vcoeff,
-                 const void *const *psi0, const int *tile, int krydim, double tol,
+                 const void *const *psi0, const int *tile, const int *team, int krydim, double tol,
                  int max_restarts, cudaStream_t st) {
     RP_REQUIRE(nprob >= 1, -2, "no problems in the batch");
     RP_REQUIRE(krydim >= 2 && krydim <= BMAXK, -2, "batched krydim must be in [2, 32]");
@@ -469,12 +580,17 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
     bp.hcap = max_restarts * krydim;
     bp.plans.resize(nprob);
     std::vector<BatchProblem> probs(nprob);
+    std::vector<int> teams(nprob);
     for (int p = 0; p < nprob; p++) {
         RP_REQUIRE(len[p] >= 8 && len[p] <= 30, -2, "batched problems need 8..30 qubits");
         RP_REQUIRE(psi0[p] && ((uintptr_t)psi0[p] & 15) == 0, -2, "psi0 must be 16-byte aligned");
         ApplyConfig cfg;
         int B = tile && tile[p] ? tile[p] : std::max(8, std::min(11, len[p] - 4));
         RP_REQUIRE(B >= 8 && B <= 11 && B <= len[p], -2, "batched tile exponent must be in [8, 11]");
+        const int C = team && team[p] ? team[p] : default_team(len[p]);
+        RP_REQUIRE(C == 1 || C == 2 || C == 4 || C == 8 || C == 16, -2,
+                   "batched team size must be 1, 2, 4, 8 or 16");
+        teams[p] = C;
         cfg.B = B;
         cfg.P = BT;
         cfg.stages = BST;
@@ -496,31 +612,58 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
         P.wci = (float)wcoeff[2 * p + 1];
         P.vcr = (float)vcoeff[2 * p];
         P.vci = (float)vcoeff[2 * p + 1];
-        bp.maxB = std::max(bp.maxB, B);
-        bp.maxlen = std::max(bp.maxlen, len[p]);
     }
-    // largest problems first (they take longest)
+    // classes by team size (one launch each per time step), largest problems
+    // first inside a class (they take longest)
     bp.order.resize(nprob);
     for (int p = 0; p < nprob; p++) bp.order[p] = p;
-    std::stable_sort(bp.order.begin(), bp.order.end(),
-                     [&](int x, int y) { return probs[x].len > probs[y].len; });
+    std::stable_sort(bp.order.begin(), bp.order.end(), [&](int x, int y) {
+        if (teams[x] != teams[y]) return teams[x] > teams[y];
+        return probs[x].len > probs[y].len;
+    });
     for (int i = 0; i < nprob; i++) bp.probs.push_back(probs[bp.order[i]]);
+    for (int i = 0; i < nprob; i++) {
+        const int p = bp.order[i];
+        if (bp.classes.empty() || bp.classes.back().team != teams[p]) {
+            BatchClass c;
+            c.team = teams[p];
+            c.first = i;
+            bp.classes.push_back(c);
+        }
+        BatchClass &c = bp.classes.back();
+        c.count++;
+        c.maxB = std::max(c.maxB, probs[p].B);
+        c.maxlen = std::max(c.maxlen, probs[p].len);
+    }
     RP_CUDA(cudaMalloc((void **)&bp.d_probs, nprob * sizeof(BatchProblem)));
     RP_CUDA(cudaMemcpy(bp.d_probs, bp.probs.data(), nprob * sizeof(BatchProblem),
                        cudaMemcpyHostToDevice));
-    // one workspace slot per resident CTA
-    const size_t smem = dyn_smem(bp.maxB, bp.hcap);
+    // one workspace slot per resident team; the classes run one after the
+    // other, so they share the allocation
+    int maxB = 8;
+    for (auto &c : bp.classes) maxB = std::max(maxB, c.maxB);
+    const size_t smem_max = dyn_smem(maxB, bp.hcap);
     RP_CUDA(cudaFuncSetAttribute(k_batch_otoc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    int per_sm = 0;
-    RP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_otoc, BT, smem));
-    RP_REQUIRE(per_sm >= 1, -2, "batched kernel does not fit on an SM");
-    bp.nslots = std::min(nprob, per_sm * num_sms());
-    bp.vec_stride = (((size_t)1 << bp.maxlen) * sizeof(Cplx<float>) + 255) & ~(size_t)255;
-    const size_t small = ((size_t)krydim * krydim + (size_t)bp.hcap * bp.hcap +
-                          10 * (size_t)bp.hcap * bp.hcap) * sizeof(cd);
-    bp.ws_stride = (((size_t)(krydim + 4) * bp.vec_stride + small) + 255) & ~(size_t)255;
-    cudaError_t e = cudaMalloc(&bp.ws, bp.ws_stride * bp.nslots);
+                                 (int)smem_max));
+    RP_CUDA(cudaFuncSetAttribute(k_batch_otoc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    size_t ws_bytes = 0;
+    for (auto &c : bp.classes) {
+        c.smem = dyn_smem(c.maxB, bp.hcap);
+        cudaLaunchAttribute attr[1];
+        BatchClass probe = c;
+        probe.nslots = 1;
+        cudaLaunchConfig_t cfg = class_config(probe, c.smem, st, attr);
+        int nclusters = 0;
+        RP_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, k_batch_otoc, &cfg));
+        RP_REQUIRE(nclusters >= 1, -2, "a batched team of this size does not fit on the GPU");
+        c.nslots = std::min(nclusters, c.count);
+        c.vec_stride = (((size_t)1 << c.maxlen) * sizeof(Cplx<float>) + 255) & ~(size_t)255;
+        const size_t small = ((size_t)krydim * krydim + (size_t)bp.hcap * bp.hcap +
+                              10 * (size_t)bp.hcap * bp.hcap) * sizeof(cd);
+        c.ws_stride = (((size_t)(krydim + 4) * c.vec_stride + small) + 255) & ~(size_t)255;
+        ws_bytes = std::max(ws_bytes, c.ws_stride * c.nslots);
+    }
+    cudaError_t e = cudaMalloc(&bp.ws, ws_bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         batch_free(bp);
@@ -528,44 +671,64 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
     }
     RP_CUDA(cudaMalloc((void **)&bp.err, sizeof(unsigned)));
     RP_CUDA(cudaMemset(bp.err, 0, sizeof(unsigned)));
-    (void)st;
+}
+
+static BatchArgs class_args(const BatchPlan &bp, const BatchClass &c, int ntimes) {
+    BatchArgs a{};
+    a.probs = bp.d_probs + c.first;
+    a.nprob = c.count;
+    a.out_base = c.first;
+    a.krydim = bp.krydim;
+    a.max_restarts = bp.max_restarts;
+    a.ntimes = ntimes;
+    a.hcap = bp.hcap;
+    a.tol = bp.tol;
+    a.F = bp.F;
+    a.applies = bp.applies;
+    a.ws = static_cast<char *>(bp.ws);
+    a.ws_stride = c.ws_stride;
+    a.vec_stride = c.vec_stride;
+    a.err = bp.err;
+    return a;
+}
+
+static void ensure_outputs(BatchPlan &bp, int ntimes) {
+    if (ntimes <= bp.ntimes_cap) return;
+    if (bp.counter) cudaFree(bp.counter);
+    if (bp.F) cudaFree(bp.F);
+    if (bp.applies) cudaFree(bp.applies);
+    bp.counter = nullptr;
+    bp.F = nullptr;
+    bp.applies = nullptr;
+    const size_t nc = bp.classes.size();
+    RP_CUDA(cudaMalloc((void **)&bp.counter, nc * ntimes * sizeof(int)));
+    RP_CUDA(cudaMalloc((void **)&bp.F, (size_t)bp.nprob * ntimes * 2 * sizeof(double)));
+    RP_CUDA(cudaMalloc((void **)&bp.applies, (size_t)bp.nprob * ntimes * sizeof(int)));
+    bp.ntimes_cap = ntimes;
+    if (bp.graph) cudaGraphExecDestroy(bp.graph);
+    bp.graph = nullptr;
 }
 
 double batch_probe(BatchPlan &bp, int napplies, cudaStream_t st) {
     RP_REQUIRE(napplies >= 1 && napplies <= 64, -2, "napplies must be in [1, 64]");
-    const double zero = 0.0;
-    BatchArgs a{};
-    if (bp.ntimes_cap < 1) {
-        RP_CUDA(cudaMalloc((void **)&bp.counter, sizeof(int)));
-        RP_CUDA(cudaMalloc((void **)&bp.F, (size_t)bp.nprob * 2 * sizeof(double)));
-        RP_CUDA(cudaMalloc((void **)&bp.applies, (size_t)bp.nprob * sizeof(int)));
-        bp.ntimes_cap = 1;
-    }
-    a.probs = bp.d_probs;
-    a.nprob = bp.nprob;
-    a.krydim = bp.krydim;
-    a.max_restarts = bp.max_restarts;
-    a.ntimes = 1;
-    a.hcap = bp.hcap;
-    a.tol = bp.tol;
-    a.t = zero;
-    a.probe = napplies;
-    a.F = bp.F;
-    a.applies = bp.applies;
-    a.ws = static_cast<char *>(bp.ws);
-    a.ws_stride = bp.ws_stride;
-    a.vec_stride = bp.vec_stride;
-    a.counter = bp.counter;
-    a.err = bp.err;
-    const size_t smem = dyn_smem(bp.maxB, bp.hcap);
+    ensure_outputs(bp, 1);
     cudaEvent_t e0, e1;
     RP_CUDA(cudaEventCreate(&e0));
     RP_CUDA(cudaEventCreate(&e1));
     RP_CUDA(cudaMemsetAsync(bp.err, 0, sizeof(unsigned), st));
-    RP_CUDA(cudaMemsetAsync(bp.counter, 0, sizeof(int), st));
+    RP_CUDA(cudaMemsetAsync(bp.counter, 0, bp.classes.size() * sizeof(int), st));
     RP_CUDA(cudaEventRecord(e0, st));
-    k_batch_otoc<<<bp.nslots, BT, smem, st>>>(a);
-    RP_CUDA(cudaGetLastError());
+    for (size_t ci = 0; ci < bp.classes.size(); ci++) {
+        const BatchClass &c = bp.classes[ci];
+        BatchArgs a = class_args(bp, c, 1);
+        a.t = 0.0;
+        a.ti = 0;
+        a.probe = napplies;
+        a.counter = bp.counter + ci;
+        cudaLaunchAttribute attr[1];
+        cudaLaunchConfig_t cfg = class_config(c, c.smem, st, attr);
+        RP_CUDA(cudaLaunchKernelEx(&cfg, k_batch_otoc, a));
+    }
     RP_CUDA(cudaEventRecord(e1, st));
     unsigned herr = 0;
     RP_CUDA(cudaMemcpyAsync(&herr, bp.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -581,40 +744,21 @@ double batch_probe(BatchPlan &bp, int napplies, cudaStream_t st) {
 void batch_otoc(BatchPlan &bp, int ntimes, const double *times, double *F_host,
                 int *applies_host, int use_graph, cudaStream_t st) {
     RP_REQUIRE(ntimes >= 1, -2, "no time points");
-    if (ntimes > bp.ntimes_cap) {
-        if (bp.counter) cudaFree(bp.counter);
-        if (bp.F) cudaFree(bp.F);
-        if (bp.applies) cudaFree(bp.applies);
-        RP_CUDA(cudaMalloc((void **)&bp.counter, ntimes * sizeof(int)));
-        RP_CUDA(cudaMalloc((void **)&bp.F, (size_t)bp.nprob * ntimes * 2 * sizeof(double)));
-        RP_CUDA(cudaMalloc((void **)&bp.applies, (size_t)bp.nprob * ntimes * sizeof(int)));
-        bp.ntimes_cap = ntimes;
-        if (bp.graph) cudaGraphExecDestroy(bp.graph);
-        bp.graph = nullptr;
-    }
-    const size_t smem = dyn_smem(bp.maxB, bp.hcap);
-    BatchArgs a{};
-    a.probs = bp.d_probs;
-    a.nprob = bp.nprob;
-    a.krydim = bp.krydim;
-    a.max_restarts = bp.max_restarts;
-    a.ntimes = ntimes;
-    a.hcap = bp.hcap;
-    a.tol = bp.tol;
-    a.F = bp.F;
-    a.applies = bp.applies;
-    a.ws = static_cast<char *>(bp.ws);
-    a.ws_stride = bp.ws_stride;
-    a.vec_stride = bp.vec_stride;
-    a.counter = bp.counter;
-    a.err = bp.err;
+    ensure_outputs(bp, ntimes);
+    const size_t nc = bp.classes.size();
     auto enqueue = [&](cudaStream_t s) {
-        RP_CUDA(cudaMemsetAsync(bp.counter, 0, ntimes * sizeof(int), s));
+        RP_CUDA(cudaMemsetAsync(bp.counter, 0, nc * ntimes * sizeof(int), s));
         for (int k = 0; k < ntimes; k++) {
-            a.t = times[k];
-            a.ti = k;
-            k_batch_otoc<<<bp.nslots, BT, smem, s>>>(a);
-            RP_CUDA(cudaGetLastError());
+            for (size_t ci = 0; ci < nc; ci++) {
+                const BatchClass &c = bp.classes[ci];
+                BatchArgs a = class_args(bp, c, ntimes);
+                a.t = times[k];
+                a.ti = k;
+                a.counter = bp.counter + ci * ntimes;
+                cudaLaunchAttribute attr[1];
+                cudaLaunchConfig_t cfg = class_config(c, c.smem, s, attr);
+                RP_CUDA(cudaLaunchKernelEx(&cfg, k_batch_otoc, a));
+            }
         }
     };
     RP_CUDA(cudaMemsetAsync(bp.err, 0, sizeof(unsigned), st));

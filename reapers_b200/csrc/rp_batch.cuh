@@ -18,17 +18,23 @@ struct alignas(16) BatchProblem {
     float wcr, wci, vcr, vci;       // their coefficients
 };
 
+// Problems sharing a team size: one persistent launch per time step, teams
+// (clusters of `team` CTAs) of which `nslots` are resident.
+struct BatchClass {
+    int team = 1, first = 0, count = 0, nslots = 0, maxB = 8, maxlen = 0;
+    size_t smem = 0, ws_stride = 0, vec_stride = 0;
+};
+
 struct BatchPlan {
     int nprob = 0, krydim = 0, max_restarts = 0, hcap = 0;
     double tol = 0;
-    int maxB = 0, maxlen = 0, nslots = 0;
+    std::vector<BatchClass> classes;         // in launch order
     std::vector<ApplyPlan> plans;            // per problem (host tables + device copies)
-    std::vector<BatchProblem> probs;         // device-pointer records, largest first
+    std::vector<BatchProblem> probs;         // device-pointer records, by class, largest first
     std::vector<int> order;                  // probs[i] is problem order[i]
     BatchProblem *d_probs = nullptr;
-    void *ws = nullptr;                      // per-slot workspaces
-    size_t ws_stride = 0, vec_stride = 0;
-    int *counter = nullptr;                  // work queue heads, one per time index
+    void *ws = nullptr;                      // per-team workspaces (shared by the classes)
+    int *counter = nullptr;                  // work queue heads [class][time index]
     double *F = nullptr;                     // [nprob][ntimes][2]
     int *applies = nullptr;                  // [nprob][ntimes]
     unsigned *err = nullptr;
@@ -39,16 +45,18 @@ struct BatchPlan {
 
 // Problem p: len[p] qubits, nterms[p] terms (bits, coeff as for rp_ham_create),
 // W and V single strings, psi0[p] a device complex64 vector, tile[p] the tile
-// exponent (8..12, 0 = default).
+// exponent (8..11, 0 = default), team[p] the CTAs per problem (1, 2, 4, 8 or
+// 16; 0 = default); tile and team may be null.
 void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms,
                  const uint64_t *const *bits, const double *const *coeff, const uint64_t *wbits,
                  const double *wcoeff, const uint64_t *vbits, const double *vcoeff,
-                 const void *const *psi0, const int *tile, int krydim, double tol,
-                 int max_restarts, cudaStream_t st);
+                 const void *const *psi0, const int *tile, const int *team, int krydim,
+                 double tol, int max_restarts, cudaStream_t st);
 void batch_free(BatchPlan &bp);
 
 // F[p][k] = <psi0| W(t_k) V W(t_k) V |psi0> for every problem; one persistent
-// launch per time step, captured once into a CUDA graph when use_graph.
+// launch per time step and team size, captured once into a CUDA graph when
+// use_graph.
 void batch_otoc(BatchPlan &bp, int ntimes, const double *times, double *F_host,
                 int *applies_host, int use_graph, cudaStream_t st);
 

@@ -465,6 +465,15 @@ int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nte
                     const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
                     const double *vcoeff, const void *const *psi0, const int *tile, int krydim,
                     double tol, int max_restarts) {
+    return rp_batch_create_ex(b, nprob, len, nterms, bits, coeff, wbits, wcoeff, vbits, vcoeff,
+                              psi0, tile, nullptr, krydim, tol, max_restarts);
+}
+
+int rp_batch_create_ex(rp_batch_t *b, int nprob, const int *len, const int64_t *nterms,
+                       const uint64_t *const *bits, const double *const *coeff,
+                       const uint64_t *wbits, const double *wcoeff, const uint64_t *vbits,
+                       const double *vcoeff, const void *const *psi0, const int *tile,
+                       const int *team, int krydim, double tol, int max_restarts) {
     return guarded([&] {
         RP_REQUIRE(b && len && nterms && bits && coeff && wbits && wcoeff && vbits && vcoeff &&
                        psi0,
@@ -472,7 +481,7 @@ int rp_batch_create(rp_batch_t *b, int nprob, const int *len, const int64_t *nte
         rp_batch *B = new rp_batch;
         try {
             batch_build(B->plan, nprob, len, nterms, bits, coeff, wbits, wcoeff, vbits, vcoeff,
-                        psi0, tile, krydim, tol, max_restarts, g_stream);
+                        psi0, tile, team, krydim, tol, max_restarts, g_stream);
         } catch (...) {
             delete B;
             throw;

@@ -1,5 +1,6 @@
-"""Batched OTOC (one persistent launch per time step, uneven qubit counts)
-against the FP64 CPU oracle and the single-problem mixed path.
+"""Batched OTOC (one persistent launch per time step and team size, uneven
+qubit counts) against the FP64 CPU oracle and the single-problem mixed path;
+teams of 1..16 CTAs (thread-block clusters) per problem give the same answer.
 
 Tolerance: 2e-5 absolute on the OTOC (|F(0)| = 1/4), the FP32 state storage
 of the batched form; graph replay and direct launches agree exactly."""
@@ -63,5 +64,49 @@ def test_batched_matches_single_problem_mixed_path(cuda):
 def test_batched_rejects_bad_tile(cuda):
     probs, _ = make_problems([(16, 4)])
     probs[0]["tile"] = 12
+    with pytest.raises(rb.RPError):
+        rb.BatchOTOC(probs)
+
+
+@pytest.mark.parametrize("team", [1, 2, 4, 8, 16])
+def test_batched_team_sizes_agree(cuda, team):
+    """One problem shared by a cluster of `team` CTAs: same OTOC as the oracle
+    and as one CTA, within FP32 rounding; same H.psi count."""
+    specs = [(20, 4), (18, 4), (16, 4)]
+    probs, refs = make_problems(specs, seed=11)
+    times = np.array([0.0, 0.8])
+    ref_b = rb.BatchOTOC([dict(p, team=1) for p in probs], krydim=10, tol=1e-7, max_restarts=16)
+    F1, ap1 = ref_b.run(times)
+    ref_b.close()
+    b = rb.BatchOTOC([dict(p, team=team) for p in probs], krydim=10, tol=1e-7, max_restarts=16)
+    F, ap = b.run(times, use_graph=True)
+    F2, _ = b.run(times, use_graph=False)
+    b.close()
+    assert np.array_equal(F, F2)
+    assert np.abs(F - F1).max() < 2e-6
+    assert np.abs(ap - ap1).max() <= 10
+    for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
+        ref = O.otoc(L, bits, coeff, w, v, psi, times, 10, 1e-12)
+        assert np.abs(F[p] - ref).max() < 2e-5, (p, F[p], ref)
+
+
+def test_batched_mixed_team_classes(cuda):
+    """Problems of different team sizes in one batch: one launch per class."""
+    specs = [(16, 4), (20, 4), (18, 4), (20, 4)]
+    probs, refs = make_problems(specs, seed=21)
+    for p, t in zip(probs, [1, 16, 4, 8]):
+        p["team"] = t
+    times = np.array([0.7])
+    b = rb.BatchOTOC(probs, krydim=10, tol=1e-7, max_restarts=16)
+    F, ap = b.run(times)
+    b.close()
+    for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
+        ref = O.otoc(L, bits, coeff, w, v, psi, times, 10, 1e-12)
+        assert np.abs(F[p] - ref).max() < 2e-5, (p, F[p], ref)
+
+
+def test_batched_rejects_bad_team(cuda):
+    probs, _ = make_problems([(16, 4)])
+    probs[0]["team"] = 3
     with pytest.raises(rb.RPError):
         rb.BatchOTOC(probs)
