@@ -63,6 +63,7 @@ struct BatchShared {
     Cplx<float> *u[BMAXK + 1];
     int item;
     int pbuf;                     // which part[] buffer the next reduction uses
+    int abort;                    // the ring's producer gave up (bounded wait)
 };
 
 __device__ __forceinline__ void proxy_fence_global() {
@@ -198,52 +199,63 @@ __device__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double 
 }
 
 // out = scale * H in over the team's output tiles (rank, rank + C, ...),
-// source tiles streamed through this CTA's shared-memory ring.  git counts
-// ring items across calls (stage = git % BST, parity (git/BST)&1).  Returns
-// false in every CTA of the team if a bounded wait gave up in any of them.
+// source tiles streamed through this CTA's shared-memory ring: full[s]
+// completes when the bulk copy into stage s lands, empty[s] when every warp
+// is done with it.  Thread 0 issues item i + BST - 1 after the warps released
+// item i - 1, so warps run up to BST - 1 items apart without CTA barriers.
+// git counts ring items across calls (stage = git % BST, parity (git/BST)&1).
+// Returns false in every CTA of the team if a bounded wait gave up in any.
 template <int B>
 __device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, const Cplx<float> *in,
-                           Cplx<float> *out, double scale, unsigned char *stages, uint64_t *full,
-                           long &git, BatchShared &S, unsigned *err) {
+                                        Cplx<float> *out, double scale, unsigned char *stages,
+                                        uint64_t *full, uint64_t *empty, long &git, BatchShared &S,
+                                        unsigned *err) {
     constexpr int TILE = 1 << B, E = TILE / BT;
     constexpr unsigned TB = TILE * sizeof(Cplx<float>);
     const int my_tiles = P.ntiles > (int)tm.rank ? (P.ntiles - 1 - (int)tm.rank) / (int)tm.size + 1 : 0;
     const long total = (long)my_tiles * P.ngroups;
-    const uint32_t t = threadIdx.x;
+    const uint32_t t = threadIdx.x, lane = t & 31;
     const uint64_t keep = l2_policy_evict_last();   // the input is re-read once per group
-    auto issue = [&](long i) {
+    long issued = 0;                                // thread 0 only
+    // item i into its stage, once the warps have released the stage's previous item
+    auto issue = [&](long i) -> bool {
         const long gi = git + i;
         const int s = (int)(gi % BST);
+        if (gi >= BST && !mbar_wait_bounded(&empty[s], (unsigned)(((gi / BST) - 1) & 1), err))
+            return false;
         const int o = (int)tm.rank + (int)(i / P.ngroups) * (int)tm.size, g = (int)(i % P.ngroups);
         const uint32_t src = (uint32_t)o ^ P.groups[g].xh;
         mbar_arrive_expect_tx(&full[s], TB);
         bulk_g2s_hint(stages + (size_t)s * TB, in + ((size_t)src << B), TB, &full[s], keep);
+        issued = i + 1;
+        return true;
     };
     if (t == 0) {
+        S.abort = 0;
         proxy_fence_global();
-        for (long i = 0; i < BST - 1 && i < total; i++) issue(i);
+        for (long i = 0; i < BST - 1 && i < total; i++)
+            if (!issue(i)) {
+                S.abort = 1;
+                break;
+            }
     }
+    __syncthreads();
     bool ok = true;
     float ar[E], ai[E];
-    for (long it = 0; it < total; ++it) {
+    long it = 0;
+    for (; it < total; ++it) {
         const long gi = git + it;
         const int s = (int)(gi % BST);
         const unsigned par = (unsigned)((gi / BST) & 1);
-        const int o = (int)tm.rank + (int)(it / P.ngroups) * (int)tm.size;
-        const int g = (int)(it % P.ngroups);
+        if (t == 0 && it + BST - 1 < total && !S.abort)
+            if (!issue(it + BST - 1)) S.abort = 1;
         const bool okw = mbar_wait_bounded(&full[s], par, err);
-        if (!__syncthreads_and(okw)) {
-            // drain the copies still in flight, then stop this CTA's share
-            if (t == 0)
-                for (long i = it; i < it + BST - 1 && i < total; i++)
-                    mbar_wait_bounded(&full[(git + i) % BST], (unsigned)(((git + i) / BST) & 1), err);
-            __syncthreads();
+        if (!__all_sync(0xffffffffu, okw && *(volatile int *)&S.abort == 0)) {
             ok = false;
             break;
         }
-        // every thread is past this item's barrier, so the stage of item it-1
-        // is free: prefetch item it + BST - 1 into it
-        if (t == 0 && it + BST - 1 < total) issue(it + BST - 1);
+        const int o = (int)tm.rank + (int)(it / P.ngroups) * (int)tm.size;
+        const int g = (int)(it % P.ngroups);
         if (g == 0) {
 #pragma unroll
             for (int j = 0; j < E; j++) ar[j] = ai[j] = 0.f;
@@ -278,6 +290,8 @@ __device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, c
                 }
             }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
         if (g == P.ngroups - 1) {
             Cplx<float> *op = out + ((size_t)o << B) + t;
 #pragma unroll
@@ -285,6 +299,12 @@ __device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, c
                 op[(size_t)j * BT] = Cplx<float>{(float)(scale * ar[j]), (float)(scale * ai[j])};
         }
     }
+    if (!ok && t == 0) {
+        // let every copy already issued land before the stages are reused
+        for (long i = it; i < issued; i++)
+            mbar_wait_bounded(&full[(git + i) % BST], (unsigned)(((git + i) / BST) & 1), err);
+    }
+    __syncthreads();
     git += total;
     proxy_fence_global();
     return team_and(tm, ok, S);
@@ -294,8 +314,8 @@ __device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, c
 template <int B>
 __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *psi,
                             double t_real, const BatchArgs &a, char *slot, BatchShared &S,
-                            unsigned char *stages, uint64_t *full, double *esmem, long &git,
-                            int &applies) {
+                            unsigned char *stages, uint64_t *full, uint64_t *empty, double *esmem,
+                            long &git, int &applies) {
     if (t_real == 0.0) return true;   // State::evolve returns at t = beta = 0
     const uint32_t n = 1u << P.len;
     const int m = a.krydim;
@@ -335,7 +355,7 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
         bool brokedown = false;
         for (int j = 0; j < m; j++) {
             Cplx<float> *w = S.u[j + 1];
-            if (!team_apply<B>(tm, P, S.u[j], w, S.sigma[j], stages, full, git, S, a.err))
+            if (!team_apply<B>(tm, P, S.u[j], w, S.sigma[j], stages, full, empty, git, S, a.err))
                 return false;
             applies++;
             double old = 1.0, norm = eta / 2;
@@ -440,8 +460,8 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
 template <int B>
 __device__ __noinline__ bool team_otoc(const Team &tm, const BatchProblem &P, const BatchArgs &a,
                                        char *slot, BatchShared &S, unsigned char *stages,
-                                       uint64_t *full, double *esmem, long &git, int &applies,
-                                       double &fr, double &fi) {
+                                       uint64_t *full, uint64_t *empty, double *esmem, long &git,
+                                       int &applies, double &fr, double &fi) {
     const uint32_t n = 1u << P.len;
     Cplx<float> *psi = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 2) * a.vec_stride);
     Cplx<float> *tmp = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 3) * a.vec_stride);
@@ -450,20 +470,20 @@ __device__ __noinline__ bool team_otoc(const Team &tm, const BatchProblem &P, co
         team_copy(tm, psi, P.psi0, n);
         for (int r = 0; r < a.probe; r++) {
             if (!team_apply<B>(tm, P, (r & 1) ? tmp : psi, (r & 1) ? psi : tmp, 1.0, stages, full,
-                               git, S, a.err))
+                               empty, git, S, a.err))
                 return false;
             applies++;
         }
         return true;
     }
     team_string(tm, P.vx, P.vz, P.vcr, P.vci, P.psi0, psi, n);
-    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
     team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
     team_string(tm, P.vx, P.vz, P.vcr, P.vci, tmp, psi, n);
-    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
     team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
     team_dot(tm, P.psi0, tmp, n, S, fr, fi);
     return true;
 }
@@ -472,14 +492,19 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ BatchShared S;
     __shared__ __align__(8) uint64_t full[BST];
+    __shared__ __align__(8) uint64_t empty[BST];
     unsigned char *stages = dsm;
     double *esmem = nullptr;
     cg::cluster_group cl = cg::this_cluster();
     const Team tm{cl.block_rank(), cl.num_blocks()};
     if (threadIdx.x == 0) {
-        for (int s = 0; s < BST; s++) mbar_init(&full[s], 1);
+        for (int s = 0; s < BST; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], BNW);
+        }
         fence_barrier_init();
         S.pbuf = 0;
+        S.abort = 0;
     }
     __syncthreads();
     long git = 0;
@@ -498,10 +523,10 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
         double fr = 0.0, fi = 0.0;
         bool ok = false;
         switch (P.B) {
-            case 8: ok = team_otoc<8>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            case 9: ok = team_otoc<9>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            case 10: ok = team_otoc<10>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
-            default: ok = team_otoc<11>(tm, P, a, slot, S, stages, full, esmem, git, applies, fr, fi); break;
+            case 8: ok = team_otoc<8>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
+            case 9: ok = team_otoc<9>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
+            case 10: ok = team_otoc<10>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
+            default: ok = team_otoc<11>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
         }
         if (!ok) break;   // identical in every CTA of the team
         if (tm.rank == 0 && threadIdx.x == 0) {
