@@ -173,8 +173,8 @@ int rp_arnoldi(rp_ham_t h, const void *psi, int m, double *H, rp_arnoldi_info_t 
  * (coef: 2*m_eff doubles, complex interleaved). */
 int rp_arnoldi_combine(const double *coef, void *out);
 /* For c < ncand: col0[c] = first column of exp((fr[c] + i fi[c]) H), H m x m
- * complex column-major; FP64 Pade-13 on the GPU, one CTA per candidate
- * (col0: 2*m*ncand doubles). */
+ * complex column-major, m <= 1024, ncand <= 64; FP64 Pade-13 on the GPU,
+ * one CTA per candidate (col0: 2*m*ncand doubles). */
 int rp_expm_first_column(int m, const double *H, int ncand, const double *fr, const double *fi,
                          double *col0);
 

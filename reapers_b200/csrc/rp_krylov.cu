@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(256) k_expm_cands(int m, const cd *H, const do
 
 void expm_candidates(int m, const double *H, int ncand, const double *fr, const double *fi,
                      double *col0, cudaStream_t st) {
-    RP_REQUIRE(m >= 1 && m <= 256 && ncand >= 1 && ncand <= 64, -2, "bad expm batch size");
+    RP_REQUIRE(m >= 1 && m <= 1024 && ncand >= 1 && ncand <= 64, -2, "bad expm batch size");
     const size_t hb = (size_t)m * m * sizeof(cd);
     const size_t sb = (size_t)ncand * 10 * m * m * sizeof(cd);
     const size_t need = hb + sb + 2 * ncand * sizeof(double) + (size_t)ncand * m * sizeof(cd);
