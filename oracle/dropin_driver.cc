@@ -10,7 +10,8 @@
 // oracle/_ref/dropin_driver; run by tests/test_gpu_dropin.py.
 //
 // usage: dropin_driver N sparsity seed t krydim
-// prints one JSON object of relative differences (GPU backend vs CPU backend).
+// prints one JSON object of relative differences (GPU backend vs CPU backend)
+// and both backends' ground-state energies.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -147,11 +148,21 @@ int main(int argc, char **argv) {
     GSt g5 = ham_g * g0;
     const double mutate = rel_diff(g5, c5);
 
+    // the reference's ground-state Lanczos (inc/algo.h:180-257) on both
+    // backends; the random starting states differ, the answers must not
+    CSt gc(L);
+    GSt gg(L);
+    const double Ec = gc.ground_state(ham_c, 20, 1e-10, 400);
+    const double Eg = gg.ground_state(ham_g, 20, 1e-10, 400);
+    CSt ggh(gg);
+    const double overlap = std::abs(gc * ggh);
+
     std::printf(
         "{\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
         "\"apply\": %.3e, \"evolve_ref_krylov\": %.3e, \"evolve_b200krylov\": %.3e, "
-        "\"evolve_beta\": %.3e, \"otoc\": %.3e, \"F\": [%.12e, %.12e], \"mutate\": %.3e}\n",
+        "\"evolve_beta\": %.3e, \"otoc\": %.3e, \"F\": [%.12e, %.12e], \"mutate\": %.3e, "
+        "\"E0_cpu\": %.15e, \"E0_b200\": %.15e, \"ground_overlap\": %.15f}\n",
         N, ham_c.size(), terms, roundtrip, elem, apply, evolve, evolve_fused, evolve_beta, otoc,
-        (double)Fc.real(), (double)Fc.imag(), mutate);
+        (double)Fc.real(), (double)Fc.imag(), mutate, Ec, Eg, overlap);
     return 0;
 }

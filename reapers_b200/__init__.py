@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import RP_C64, RP_C128, RPError
 from . import syk  # noqa: F401  (term generators)
 
-__all__ = ["Hamiltonian", "evolve", "dot", "norm", "axpy", "scale", "random_state",
+__all__ = ["Hamiltonian", "evolve", "ground_state", "dot", "norm", "axpy", "scale", "random_state",
            "stream", "synchronize", "RPError", "RP_C64", "RP_C128", "dtype_code", "syk",
            "otoc"]
 
@@ -131,6 +131,54 @@ def evolve(ham, psi, t, beta=0.0, krydim=5, tol=None, max_iters=0):
     _lib.call("rp_evolve", ham.handle, _ptr(psi), float(t), float(beta), int(krydim),
               float(tol), int(max_iters), C.byref(st))
     return {k: getattr(st, k) for k, _ in _lib.EvolveStats._fields_}
+
+
+def ground_state(ham, krydim=5, eps=None, maxiter=0, seed=0):
+    """(energy, state) of the lowest eigenvalue of a Hermitian H by the
+    reference's restarted Lanczos (Krylov::ground_state, inc/algo.h:180-257):
+    from a random state, krydim Lanczos steps without reorthogonalisation,
+    the tridiagonal eigenproblem on the host, restart from the Ritz vector
+    until beta_0 <= eps (default 10 machine epsilons) or maxiter iterations
+    (0 = no limit).  Vectors and H.psi on the GPU."""
+    import torch
+    from scipy.linalg import eigh_tridiagonal
+    m = int(krydim)
+    if m < 2:
+        raise ValueError("krydim must be at least 2")
+    prec = np.float32 if ham.dtype == RP_C64 else np.float64
+    if eps is None:
+        eps = 10 * float(np.finfo(prec).eps)
+    v0 = random_state(ham.len, "c64" if ham.dtype == RP_C64 else "c128", seed=seed)
+    numiter = 0
+    while True:
+        V = [v0]
+        alpha, beta = [], []
+        for i in range(m):
+            w = torch.empty_like(v0)
+            ham.apply(w, V[i])
+            alpha.append(dot(V[i], w).real)
+            if i == m - 1:
+                break
+            axpy(w, -alpha[i], V[i])
+            if i:
+                axpy(w, -beta[i - 1], V[i - 1])
+            b = norm(w)
+            if b == 0.0:          # invariant subspace: the Ritz values are exact
+                break
+            beta.append(b)
+            scale(w, 1.0 / b)
+            V.append(w)
+        k = len(alpha)
+        evals, evecs = eigh_tridiagonal(np.array(alpha), np.array(beta[:k - 1]))
+        idx = int(np.argmin(evals))
+        g = torch.zeros_like(v0)
+        for i in range(k):
+            axpy(g, float(evecs[i, idx]), V[i])
+        scale(g, 1.0 / norm(g))
+        numiter += 1
+        v0 = g
+        if not (beta and beta[0] > eps and (not maxiter or numiter < maxiter)):
+            return float(evals[idx]), g
 
 
 def dot(a, b):

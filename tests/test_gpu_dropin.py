@@ -7,8 +7,10 @@ to the sm_100a kernels -- and reports the relative difference of each result:
 the SYK term list, the host->device->host state round trip, element access,
 State operator* (H.psi), the reference's restarted Krylov evolve, the
 GPU-resident Krylov selected as State::evolve<B200Krylov>, imaginary-time
-evolution, the OTOC sequence of examples/simple-syk-krylov.cc, and an apply
-after the operator is changed (device table dropped and rebuilt).
+evolution, the OTOC sequence of examples/simple-syk-krylov.cc, an apply
+after the operator is changed (device table dropped and rebuilt), and the
+reference's ground-state Lanczos (energy; state overlap where the ground
+state is not degenerate).
 """
 import json
 import os
@@ -43,3 +45,7 @@ def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
     for k in ("apply", "evolve_ref_krylov", "evolve_b200krylov", "evolve_beta", "mutate"):
         assert d[k] <= 1e-12, (k, d)
     assert d["otoc"] <= 1e-11, d
+    # ground state (inc/algo.h:180-257) from different random starts
+    assert abs(d["E0_b200"] - d["E0_cpu"]) <= 1e-10 * abs(d["E0_cpu"]), d
+    if N % 8 == 0:   # no parity-sector degeneracy: the same state up to a phase
+        assert d["ground_overlap"] >= 1 - 1e-8, d
