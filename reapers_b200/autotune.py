@@ -4,7 +4,8 @@ For every distinct (qubit count, number of source-tile groups, precision,
 Krylov dimension) in a batch, the tuner times one persistent launch doing
 two H.psi products per problem (rp_batch_probe) on a sample of the batch's
 own problems of that size (up to one per SM, so the memory system is loaded
-as in the real run), for each tile exponent B in 8..min(11, L) and each
+as in the real run), for each tile exponent B in 8..min(12, L) (12: the
+row-tile loop) and each
 team size (CTAs per problem, a thread-block cluster) C in 1, 2, 4, 8, 16
 with C <= 2^(L-B) tiles, and keeps the fastest pair.  Results are cached in
 a JSON file (``RPB200_TUNE_CACHE`` or ``~/.cache/reapers_b200/tune.json``)
@@ -69,7 +70,7 @@ def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, sample=None,
             L = int(problems[idx[0]]["len"])
             n = sample or min(len(idx), sms)
             timings = {}
-            for B in range(8, min(11, L) + 1):
+            for B in range(8, min(12, L) + 1):
                 for C in (1, 2, 4, 8, 16):
                     if C > (1 << (L - B)):
                         continue

@@ -29,6 +29,7 @@
 
 #include "rp_apply.cuh"
 #include "rp_apply_rows.cuh"
+#include "rp_rows_dev.cuh"
 
 namespace rp {
 
@@ -39,7 +40,7 @@ static int log2i(uint64_t v) {
 }
 
 void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
-                   int64_t nterms) {
+                   int64_t nterms, bool any_len) {
     rp = RowPlan{};
     const int esz = dtype == 2 ? 16 : 8;
     const int C = 128 / esz;         // elements per row
@@ -47,7 +48,9 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
     const int logC = log2i(C);
     const int logE = log2i(EPC);
     const int B = logC + 8;
-    if (len < B + 7) return;   // fewer than 128 tiles: the first-generation kernel
+    // fewer than 128 tiles: the first-generation kernel (unless the caller
+    // only needs the table, as the batched kernel does: one tile suffices)
+    if (len < (any_len ? B : B + 7)) return;
     struct T {
         uint32_t x, z;
         double c;
@@ -149,63 +152,6 @@ struct RowArgs {
     double *partials;
     unsigned *err;
 };
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// One term over a whole row.  w[p], loaded from rq ^ (p << 4), holds source
-// chunk p ^ xq (the permutation is in the address); case K = x0 | z0 << 1 | kind << 2.  Output
-// element u = EPC p + e takes source element e ^ x0 of w[p] with sign
-// (chunk sign p) * (-1)^(z0 & (e ^ x0)).
-template <typename Real, int K>
-__device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
-                                           uint32_t rq, Real c0, uint32_t jc) {
-    constexpr int EPC = 16 / (int)sizeof(Cplx<Real>);
-    constexpr int X0 = K & 1, Z0 = (K >> 1) & 1, KIND = K >> 2;
-    if constexpr (EPC == 1 && (X0 || Z0)) {
-        return;
-    } else {
-        const Real cn = -c0;
-        float4 w[8];
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(w[p].x), "=f"(w[p].y), "=f"(w[p].z), "=f"(w[p].w)
-                         : "r"(rq ^ ((uint32_t)p << 4)));
-        }
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            const Real cp = ((jc >> p) & 1u) ? cn : c0;
-#pragma unroll
-            for (int e = 0; e < EPC; e++) {
-                const int se = e ^ X0;
-                Real vx, vy;
-                if constexpr (EPC == 2) {
-                    vx = se ? w[p].z : w[p].x;
-                    vy = se ? w[p].w : w[p].y;
-                } else {
-                    vx = __hiloint2double(__float_as_int(w[p].y), __float_as_int(w[p].x));
-                    vy = __hiloint2double(__float_as_int(w[p].w), __float_as_int(w[p].z));
-                }
-                const Real c = (Z0 & se) ? -cp : cp;
-                Cplx<Real> &a = acc[EPC * p + e];
-                if (KIND == 0) {
-                    a.x = fma(c, vx, a.x);
-                    a.y = fma(c, vy, a.y);
-                } else {
-                    a.x = fma(-c, vy, a.x);
-                    a.y = fma(c, vx, a.y);
-                }
-            }
-        }
-    }
-}
 
 constexpr int ROW_P = 256;          // consumer threads = rows per tile
 constexpr int ROW_NW = ROW_P / 32;
@@ -422,7 +368,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 
 // The state viewed as rows of 128 bytes: inner dimension 32 floats (or 16
 // doubles), outer dimension D / C rows; box = one 256-row tile, 128B swizzle.
-static CUtensorMap make_row_map(const void *base, int len, int dtype) {
+CUtensorMap make_row_map(const void *base, int len, int dtype) {
     CUtensorMap m;
     const int esz = dtype == 2 ? 16 : 8;
     const int C = 128 / esz;

@@ -1,6 +1,8 @@
 // Row-layout H.psi kernel (second generation): host-side table and launch.
 #pragma once
 
+#include <cuda.h>
+
 #include <vector>
 
 #include "rp_common.cuh"
@@ -47,8 +49,10 @@ struct RowPlan {
 constexpr int ROW_MAX_TERMS = 2048;
 constexpr int ROW_MAX_GROUPS = 1024;
 
+// any_len: build the table for any len >= the tile exponent (the batched
+// kernel); otherwise only for states of at least 128 tiles.
 void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
-                   int64_t nterms);
+                   int64_t nterms, bool any_len = false);
 void rowplan_upload(RowPlan &rp);
 void rowplan_free(RowPlan &rp);
 
@@ -66,5 +70,9 @@ struct RowLaunch {
 };
 
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st);
+
+// 2-D TMA map of a state of 2^len elements at base (rows of 128 bytes, one
+// 256-row tile per box, 128-byte swizzle).
+CUtensorMap make_row_map(const void *base, int len, int dtype);
 
 }  // namespace rp

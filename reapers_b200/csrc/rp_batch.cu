@@ -30,6 +30,7 @@
 
 #include "rp_batch.cuh"
 #include "rp_expm_impl.cuh"
+#include "rp_rows_dev.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -39,6 +40,10 @@ constexpr int BT = 256;          // threads per CTA
 constexpr int BNW = BT / 32;
 constexpr int BST = 4;           // shared-memory stages of the H.psi ring
 constexpr int BMAXK = 32;        // largest krydim of the batched form
+constexpr int RB = 12;           // row-tile exponent: 256 rows x 16 complex64
+constexpr unsigned RTILE = 256u * 128u;   // bytes of a row tile
+constexpr int RS = 2;            // stages of the row-tile ring
+constexpr int RMAXT = 512;       // largest row-kernel term / group tables in shared memory
 
 struct BatchArgs {
     const BatchProblem *probs;   // this launch's problems (one team size)
@@ -51,6 +56,10 @@ struct BatchArgs {
     size_t ws_stride, vec_stride;
     int *counter;
     unsigned *err;
+    const CUtensorMap *maps;     // [team slot][vector] 2-D TMA maps (row-tile problems)
+    int nvec;                    // vectors per slot
+    size_t stage_bytes;          // ring stages (a multiple of 1024)
+    size_t table_bytes;          // row-kernel tables (0 without row-tile problems)
 };
 
 struct BatchShared {
@@ -61,6 +70,7 @@ struct BatchShared {
     double coef[2 * (BMAXK + 1)];
     double nrm;
     Cplx<float> *u[BMAXK + 1];
+    int ui[BMAXK + 1];            // slot vector index of u[i] (its TMA map)
     int item;
     int pbuf;                     // which part[] buffer the next reduction uses
     int abort;                    // the ring's producer gave up (bounded wait)
@@ -135,7 +145,7 @@ __device__ __forceinline__ bool team_and(const Team &tm, bool ok, BatchShared &S
 }
 
 // <a|b> over n elements.
-__device__ void team_dot(const Team &tm, const Cplx<float> *a, const Cplx<float> *b, uint32_t n,
+__device__ __noinline__ void team_dot(const Team &tm, const Cplx<float> *a, const Cplx<float> *b, uint32_t n,
                          BatchShared &S, double &re, double &im) {
     double sr = 0.0, si = 0.0;
     for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
@@ -176,7 +186,7 @@ __device__ void team_string(const Team &tm, uint32_t x, uint32_t z, float cr, fl
 }
 
 // w += sum_{i < nv} coef_i u_i over the team; returns ||w||^2 (team-wide).
-__device__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double *coef, int nv,
+__device__ __noinline__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double *coef, int nv,
                             Cplx<float> *w, uint32_t n, BatchShared &S) {
     double nrm = 0.0;
     for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
@@ -310,12 +320,141 @@ __device__ __noinline__ bool team_apply(const Team &tm, const BatchProblem &P, c
     return team_and(tm, ok, S);
 }
 
+// Ring state of one CTA: shared-memory stages, full / empty barriers of the
+// bulk-copy ring (tile loop) and of the row-tile ring, item counters, the
+// problem's row tables in shared memory.
+struct Ring {
+    unsigned char *stages;   // 1024-byte aligned
+    uint64_t *full, *empty, *rfull, *rempty;
+    long git, rgit;
+    const RowTerm<float> *sterms;
+    const RowGroup *sgroups;
+    RowTerm<float> *sterms_w;
+    RowGroup *sgroups_w;
+};
+
+// out = scale * H in over the team's output tiles with the row kernel's
+// layout: 4096-element tiles brought in by 2-D TMA copies with the 128-byte
+// swizzle, thread t owns row t of the output tile and applies each term to
+// its whole 128-byte row (the permutation inside the row is folded into the
+// swizzled shared-memory address; eight compile-time cases of element
+// swap, element sign and coefficient kind).  Ring protocol as team_apply.
+__device__ __noinline__ bool team_apply_rows(const Team &tm, const BatchProblem &P,
+                                             const CUtensorMap *map, Cplx<float> *out,
+                                             double scale, Ring &R, BatchShared &S,
+                                             unsigned *err) {
+    constexpr int C = 16, LOGC = 4;
+    const int ntiles = 1 << (P.len - RB);
+    const int ng = P.rngroups;
+    const int my_tiles = ntiles > (int)tm.rank ? (ntiles - 1 - (int)tm.rank) / (int)tm.size + 1 : 0;
+    const long total = (long)my_tiles * ng;
+    const uint32_t t = threadIdx.x, lane = t & 31;
+    long issued = 0;
+    auto issue = [&](long i) -> bool {
+        const long gi = R.rgit + i;
+        const int s = (int)(gi % RS);
+        if (gi >= RS && !mbar_wait_bounded(&R.rempty[s], (unsigned)(((gi / RS) - 1) & 1), err))
+            return false;
+        const int o = (int)tm.rank + (int)(i / ng) * (int)tm.size, g = (int)(i % ng);
+        const uint32_t src = (uint32_t)o ^ R.sgroups[g].xh;
+        mbar_arrive_expect_tx(&R.rfull[s], RTILE);
+        tma_load_2d(R.stages + (size_t)s * RTILE, map, 0, (int)(src * 256u), &R.rfull[s]);
+        issued = i + 1;
+        return true;
+    };
+    if (t == 0) {
+        S.abort = 0;
+        proxy_fence_global();
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+        for (long i = 0; i < RS - 1 && i < total; i++)
+            if (!issue(i)) {
+                S.abort = 1;
+                break;
+            }
+    }
+    __syncthreads();
+    bool ok = true;
+    Cplx<float> acc[C];
+    long it = 0;
+    for (; it < total; ++it) {
+        const long gi = R.rgit + it;
+        const int s = (int)(gi % RS);
+        const unsigned par = (unsigned)((gi / RS) & 1);
+        if (t == 0 && it + RS - 1 < total && !S.abort)
+            if (!issue(it + RS - 1)) S.abort = 1;
+        const bool okw = mbar_wait_bounded(&R.rfull[s], par, err);
+        if (!__all_sync(0xffffffffu, okw && *(volatile int *)&S.abort == 0)) {
+            ok = false;
+            break;
+        }
+        const int o = (int)tm.rank + (int)(it / ng) * (int)tm.size;
+        const int g = (int)(it % ng);
+        if (g == 0) {
+#pragma unroll
+            for (int u = 0; u < C; u++) acc[u].x = acc[u].y = 0.f;
+        }
+        const RowGroup gd = R.sgroups[g];
+        const uint32_t src_hi = ((uint32_t)o ^ gd.xh) << RB;
+        const uint32_t tile = smem_u32(R.stages + (size_t)s * RTILE);
+        for (uint32_t k = gd.first; k < gd.first + gd.count; ++k) {
+            const uint4 d0 = *reinterpret_cast<const uint4 *>(&R.sterms[k]);
+            const uint32_t cs = d0.x, z = d0.y, jc = d0.z;
+            const uint32_t sr = t ^ (cs & 0xFFu);
+            const uint32_t xq = (cs >> 8) & 7u;
+            const uint32_t s0 = (uint32_t)(__popc(z & (src_hi | (sr << LOGC))) & 1);
+            float c0 = __uint_as_float(d0.w);
+            if (s0) c0 = -c0;
+            const uint32_t rq = (tile + sr * 128u) | ((xq ^ (sr & 7u)) << 4);
+            switch ((cs >> 11) & 7u) {
+                case 0: chunk_case<float, 0>(acc, rq, c0, jc); break;
+                case 1: chunk_case<float, 1>(acc, rq, c0, jc); break;
+                case 2: chunk_case<float, 2>(acc, rq, c0, jc); break;
+                case 3: chunk_case<float, 3>(acc, rq, c0, jc); break;
+                case 4: chunk_case<float, 4>(acc, rq, c0, jc); break;
+                case 5: chunk_case<float, 5>(acc, rq, c0, jc); break;
+                case 6: chunk_case<float, 6>(acc, rq, c0, jc); break;
+                default: chunk_case<float, 7>(acc, rq, c0, jc); break;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&R.rempty[s]);
+        if (g == ng - 1) {
+            float4 *orow = reinterpret_cast<float4 *>(out + ((size_t)o << RB) + (size_t)t * C);
+#pragma unroll
+            for (int p = 0; p < 8; p++)
+                orow[p] = make_float4((float)(scale * acc[2 * p].x), (float)(scale * acc[2 * p].y),
+                                      (float)(scale * acc[2 * p + 1].x),
+                                      (float)(scale * acc[2 * p + 1].y));
+        }
+    }
+    if (!ok && t == 0) {
+        for (long i = it; i < issued; i++)
+            mbar_wait_bounded(&R.rfull[(R.rgit + i) % RS], (unsigned)(((R.rgit + i) / RS) & 1), err);
+    }
+    __syncthreads();
+    R.rgit += total;
+    proxy_fence_global();
+    return team_and(tm, ok, S);
+}
+
+// H.psi of slot vector `in_idx` (pointer `in`) into out, by the problem's loop.
+template <int B>
+__device__ __forceinline__ bool team_H(const Team &tm, const BatchProblem &P, const BatchArgs &a,
+                                       int in_idx, const Cplx<float> *in, Cplx<float> *out,
+                                       double scale, Ring &R, BatchShared &S) {
+    if (P.rows) {
+        const unsigned team_id = blockIdx.x / tm.size;
+        return team_apply_rows(tm, P, a.maps + (size_t)team_id * a.nvec + in_idx, out, scale, R,
+                               S, a.err);
+    }
+    return team_apply<B>(tm, P, in, out, scale, R.stages, R.full, R.empty, R.git, S, a.err);
+}
+
 // psi <- exp(-i t H) psi by the reference's restarted Krylov, run by a team.
 template <int B>
 __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *psi,
                             double t_real, const BatchArgs &a, char *slot, BatchShared &S,
-                            unsigned char *stages, uint64_t *full, uint64_t *empty, double *esmem,
-                            long &git, int &applies) {
+                            Ring &R, double *esmem, int &applies) {
     if (t_real == 0.0) return true;   // State::evolve returns at t = beta = 0
     const uint32_t n = 1u << P.len;
     const int m = a.krydim;
@@ -326,8 +465,10 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
     cd *hfull = H + m * m;
     cd *escr = hfull + (size_t)a.hcap * a.hcap;
     if (threadIdx.x == 0)
-        for (int i = 0; i <= m; i++)
+        for (int i = 0; i <= m; i++) {
             S.u[i] = reinterpret_cast<Cplx<float> *>(slot + (size_t)i * a.vec_stride);
+            S.ui[i] = i;
+        }
     __syncthreads();
     double b2, dummy;
     team_dot(tm, psi, psi, n, S, b2, dummy);
@@ -355,8 +496,7 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
         bool brokedown = false;
         for (int j = 0; j < m; j++) {
             Cplx<float> *w = S.u[j + 1];
-            if (!team_apply<B>(tm, P, S.u[j], w, S.sigma[j], stages, full, empty, git, S, a.err))
-                return false;
+            if (!team_H<B>(tm, P, a, S.ui[j], S.u[j], w, S.sigma[j], R, S)) return false;
             applies++;
             double old = 1.0, norm = eta / 2;
             int niter = 0;
@@ -448,6 +588,9 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
             Cplx<float> *tmp = S.u[0];
             S.u[0] = S.u[m];
             S.u[m] = tmp;
+            const int ti = S.ui[0];
+            S.ui[0] = S.ui[m];
+            S.ui[m] = ti;
             S.sigma[0] = S.sigma[m];
         }
         oldbeta = beta;
@@ -459,31 +602,36 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
 
 template <int B>
 __device__ __noinline__ bool team_otoc(const Team &tm, const BatchProblem &P, const BatchArgs &a,
-                                       char *slot, BatchShared &S, unsigned char *stages,
-                                       uint64_t *full, uint64_t *empty, double *esmem, long &git,
+                                       char *slot, BatchShared &S, Ring &R, double *esmem,
                                        int &applies, double &fr, double &fi) {
     const uint32_t n = 1u << P.len;
     Cplx<float> *psi = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 2) * a.vec_stride);
     Cplx<float> *tmp = reinterpret_cast<Cplx<float> *>(slot + (size_t)(a.krydim + 3) * a.vec_stride);
     const double t = a.t;
+    if (P.rows) {   // the problem's row tables into shared memory
+        for (int i = threadIdx.x; i < P.rnterms; i += BT) R.sterms_w[i] = P.rterms[i];
+        for (int i = threadIdx.x; i < P.rngroups; i += BT) R.sgroups_w[i] = P.rgroups[i];
+        __syncthreads();
+    }
     if (a.probe > 0) {   // tuning: H.psi products only
         team_copy(tm, psi, P.psi0, n);
         for (int r = 0; r < a.probe; r++) {
-            if (!team_apply<B>(tm, P, (r & 1) ? tmp : psi, (r & 1) ? psi : tmp, 1.0, stages, full,
-                               empty, git, S, a.err))
+            const bool odd = r & 1;
+            if (!team_H<B>(tm, P, a, odd ? a.krydim + 3 : a.krydim + 2, odd ? tmp : psi,
+                           odd ? psi : tmp, 1.0, R, S))
                 return false;
             applies++;
         }
         return true;
     }
     team_string(tm, P.vx, P.vz, P.vcr, P.vci, P.psi0, psi, n);
-    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, R, esmem, applies)) return false;
     team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, R, esmem, applies)) return false;
     team_string(tm, P.vx, P.vz, P.vcr, P.vci, tmp, psi, n);
-    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, psi, t, a, slot, S, R, esmem, applies)) return false;
     team_string(tm, P.wx, P.wz, P.wcr, P.wci, psi, tmp, n);
-    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, stages, full, empty, esmem, git, applies)) return false;
+    if (!team_evolve<B>(tm, P, tmp, -t, a, slot, S, R, esmem, applies)) return false;
     team_dot(tm, P.psi0, tmp, n, S, fr, fi);
     return true;
 }
@@ -493,8 +641,25 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
     __shared__ BatchShared S;
     __shared__ __align__(8) uint64_t full[BST];
     __shared__ __align__(8) uint64_t empty[BST];
-    unsigned char *stages = dsm;
-    double *esmem = nullptr;
+    __shared__ __align__(8) uint64_t rfull[RS];
+    __shared__ __align__(8) uint64_t rempty[RS];
+    // dynamic shared memory: [ring stages, 1024-byte aligned for the 128-byte
+    // swizzle][row-kernel term and group tables][the expm's factor buffer]
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
+    Ring R;
+    R.stages = base;
+    R.full = full;
+    R.empty = empty;
+    R.rfull = rfull;
+    R.rempty = rempty;
+    R.git = 0;
+    R.rgit = 0;
+    R.sterms_w = reinterpret_cast<RowTerm<float> *>(base + a.stage_bytes);
+    R.sgroups_w = reinterpret_cast<RowGroup *>(base + a.stage_bytes + (a.table_bytes ? RMAXT * sizeof(RowTerm<float>) : 0));
+    R.sterms = R.sterms_w;
+    R.sgroups = R.sgroups_w;
+    double *esmem = reinterpret_cast<double *>(base + a.stage_bytes + a.table_bytes);
     cg::cluster_group cl = cg::this_cluster();
     const Team tm{cl.block_rank(), cl.num_blocks()};
     if (threadIdx.x == 0) {
@@ -502,12 +667,15 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], BNW);
         }
+        for (int s = 0; s < RS; s++) {
+            mbar_init(&rfull[s], 1);
+            mbar_init(&rempty[s], BNW);
+        }
         fence_barrier_init();
         S.pbuf = 0;
         S.abort = 0;
     }
     __syncthreads();
-    long git = 0;
     const unsigned team_id = blockIdx.x / tm.size;
     char *slot = a.ws + (size_t)team_id * a.ws_stride;
     while (true) {
@@ -517,16 +685,14 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
         team_sync();   // the leader rewrites S.item only after everyone read it
         if (item >= a.nprob) break;
         const BatchProblem P = a.probs[item];
-        // the expm's factor buffer sits after the largest ring in use
-        esmem = reinterpret_cast<double *>(dsm + (size_t)BST * ((size_t)1 << P.B) * sizeof(Cplx<float>));
         int applies = 0;
         double fr = 0.0, fi = 0.0;
         bool ok = false;
-        switch (P.B) {
-            case 8: ok = team_otoc<8>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
-            case 9: ok = team_otoc<9>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
-            case 10: ok = team_otoc<10>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
-            default: ok = team_otoc<11>(tm, P, a, slot, S, stages, full, empty, esmem, git, applies, fr, fi); break;
+        switch (P.rows ? 11 : P.B) {
+            case 8: ok = team_otoc<8>(tm, P, a, slot, S, R, esmem, applies, fr, fi); break;
+            case 9: ok = team_otoc<9>(tm, P, a, slot, S, R, esmem, applies, fr, fi); break;
+            case 10: ok = team_otoc<10>(tm, P, a, slot, S, R, esmem, applies, fr, fi); break;
+            default: ok = team_otoc<11>(tm, P, a, slot, S, R, esmem, applies, fr, fi); break;
         }
         if (!ok) break;   // identical in every CTA of the team
         if (tm.rank == 0 && threadIdx.x == 0) {
@@ -555,6 +721,9 @@ static void split_string(uint64_t bits, int len, uint32_t &x, uint32_t &z) {
 void batch_free(BatchPlan &bp) {
     for (auto &p : bp.plans) plan_free(p);
     bp.plans.clear();
+    for (auto &r : bp.rplans) rowplan_free(r);
+    bp.rplans.clear();
+    if (bp.maps) cudaFree(bp.maps);
     if (bp.d_probs) cudaFree(bp.d_probs);
     if (bp.ws) cudaFree(bp.ws);
     if (bp.counter) cudaFree(bp.counter);
@@ -565,8 +734,20 @@ void batch_free(BatchPlan &bp) {
     bp = BatchPlan{};
 }
 
-static size_t dyn_smem(int maxB, int hcap) {
-    return (size_t)BST * ((size_t)1 << maxB) * sizeof(Cplx<float>) + (size_t)(2 * hcap + 64) * sizeof(double);
+// Dynamic shared memory of a class: the ring stages (the larger of the two
+// loops' rings in use), the row tables when a problem uses row tiles, the
+// expm's factor buffer, and slack for the 1024-byte alignment.
+static size_t stage_bytes(const BatchClass &c) {
+    size_t b = 0;
+    if (c.any_tiled) b = (size_t)BST * ((size_t)1 << c.maxB) * sizeof(Cplx<float>);
+    if (c.any_rows) b = std::max(b, (size_t)RS * RTILE);
+    return (b + 1023) & ~(size_t)1023;
+}
+static size_t table_bytes(const BatchClass &c) {
+    return c.any_rows ? (size_t)RMAXT * (sizeof(RowTerm<float>) + sizeof(RowGroup)) : 0;
+}
+static size_t dyn_smem(const BatchClass &c, int hcap) {
+    return 1024 + stage_bytes(c) + table_bytes(c) + (size_t)(2 * hcap + 64) * sizeof(double);
 }
 
 // Default team size: one CTA up to 2^16 elements, doubling per qubit above,
@@ -604,33 +785,63 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
     bp.max_restarts = max_restarts;
     bp.hcap = max_restarts * krydim;
     bp.plans.resize(nprob);
+    bp.rplans.resize(nprob);
     std::vector<BatchProblem> probs(nprob);
     std::vector<int> teams(nprob);
     for (int p = 0; p < nprob; p++) {
         RP_REQUIRE(len[p] >= 8 && len[p] <= 30, -2, "batched problems need 8..30 qubits");
         RP_REQUIRE(psi0[p] && ((uintptr_t)psi0[p] & 15) == 0, -2, "psi0 must be 16-byte aligned");
-        ApplyConfig cfg;
-        int B = tile && tile[p] ? tile[p] : std::max(8, std::min(11, len[p] - 4));
-        RP_REQUIRE(B >= 8 && B <= 11 && B <= len[p], -2, "batched tile exponent must be in [8, 11]");
+        RP_REQUIRE(nterms[p] >= 1, -2, "empty Hamiltonian in the batch");
         const int C = team && team[p] ? team[p] : default_team(len[p]);
         RP_REQUIRE(C == 1 || C == 2 || C == 4 || C == 8 || C == 16, -2,
                    "batched team size must be 1, 2, 4, 8 or 16");
         teams[p] = C;
-        cfg.B = B;
-        cfg.P = BT;
-        cfg.stages = BST;
-        cfg.allow_rows = false;
-        plan_build(bp.plans[p], len[p], 1, bits[p], coeff[p], nterms[p], cfg);
-        RP_REQUIRE(bp.plans[p].ngroups > 0, -2, "empty Hamiltonian in the batch");
-        plan_upload(bp.plans[p]);
         BatchProblem &P = probs[p];
-        P.terms = static_cast<const TermDesc<float> *>(bp.plans[p].d_terms);
-        P.groups = bp.plans[p].d_groups;
+        P = BatchProblem{};
         P.psi0 = static_cast<const Cplx<float> *>(psi0[p]);
         P.len = len[p];
-        P.B = B;
-        P.ntiles = bp.plans[p].ntiles;
-        P.ngroups = bp.plans[p].ngroups;
+        // row tiles (exponent 12) when asked for, or by default when the
+        // state has a full tile and the tables fit in shared memory
+        const int want = tile ? tile[p] : 0;
+        RP_REQUIRE(want == 0 || (want >= 8 && want <= RB), -2,
+                   "batched tile exponent must be in [8, 12]");
+        bool rows = false;
+        if ((want == RB || want == 0) && len[p] >= RB) {
+            RowPlan &rp = bp.rplans[p];
+            rowplan_build(rp, len[p], 1, bits[p], coeff[p], nterms[p], true);
+            rows = rp.ok && rp.nterms <= RMAXT && (int)rp.groups.size() <= RMAXT;
+            if (!rows) rowplan_free(rp), rp = RowPlan{};
+        }
+        RP_REQUIRE(want != RB || rows, -2,
+                   "row tiles need >= 2^12 elements and at most 512 terms and groups");
+        if (rows) {
+            RowPlan &rp = bp.rplans[p];
+            rowplan_upload(rp);
+            P.rows = 1;
+            P.rterms = static_cast<const RowTerm<float> *>(rp.d_terms);
+            P.rgroups = rp.d_groups;
+            P.rnterms = rp.nterms;
+            P.rngroups = (int)rp.groups.size();
+            P.B = RB;
+            P.ntiles = rp.ntiles;
+        } else {
+            const int B = want ? want : std::max(8, std::min(11, len[p] - 4));
+            RP_REQUIRE(B >= 8 && B <= 11 && B <= len[p], -2,
+                       "batched tile exponent must be in [8, 11] and at most the qubit count");
+            ApplyConfig cfg;
+            cfg.B = B;
+            cfg.P = BT;
+            cfg.stages = BST;
+            cfg.allow_rows = false;
+            plan_build(bp.plans[p], len[p], 1, bits[p], coeff[p], nterms[p], cfg);
+            RP_REQUIRE(bp.plans[p].ngroups > 0, -2, "empty Hamiltonian in the batch");
+            plan_upload(bp.plans[p]);
+            P.terms = static_cast<const TermDesc<float> *>(bp.plans[p].d_terms);
+            P.groups = bp.plans[p].d_groups;
+            P.B = B;
+            P.ntiles = bp.plans[p].ntiles;
+            P.ngroups = bp.plans[p].ngroups;
+        }
         split_string(wbits[p], len[p], P.wx, P.wz);
         split_string(vbits[p], len[p], P.vx, P.vz);
         P.wcr = (float)wcoeff[2 * p];
@@ -657,7 +868,12 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
         }
         BatchClass &c = bp.classes.back();
         c.count++;
-        c.maxB = std::max(c.maxB, probs[p].B);
+        if (probs[p].rows) {
+            c.any_rows = true;
+        } else {
+            c.any_tiled = true;
+            c.maxB = std::max(c.maxB, probs[p].B);
+        }
         c.maxlen = std::max(c.maxlen, probs[p].len);
     }
     RP_CUDA(cudaMalloc((void **)&bp.d_probs, nprob * sizeof(BatchProblem)));
@@ -665,15 +881,15 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
                        cudaMemcpyHostToDevice));
     // one workspace slot per resident team; the classes run one after the
     // other, so they share the allocation
-    int maxB = 8;
-    for (auto &c : bp.classes) maxB = std::max(maxB, c.maxB);
-    const size_t smem_max = dyn_smem(maxB, bp.hcap);
+    size_t smem_max = 0;
+    for (auto &c : bp.classes) smem_max = std::max(smem_max, dyn_smem(c, bp.hcap));
+    RP_REQUIRE(smem_max <= 227 * 1024, -2, "batched kernel shared memory above 227 KB");
     RP_CUDA(cudaFuncSetAttribute(k_batch_otoc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_max));
     RP_CUDA(cudaFuncSetAttribute(k_batch_otoc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     size_t ws_bytes = 0;
     for (auto &c : bp.classes) {
-        c.smem = dyn_smem(c.maxB, bp.hcap);
+        c.smem = dyn_smem(c, bp.hcap);
         cudaLaunchAttribute attr[1];
         BatchClass probe = c;
         probe.nslots = 1;
@@ -693,6 +909,24 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
         cudaGetLastError();
         batch_free(bp);
         throw Error{-4, "device out of memory for the batched workspace"};
+    }
+    // 2-D TMA maps of every workspace vector of the classes with row-tile
+    // problems (the map covers the slot's capacity, 2^maxlen elements)
+    std::vector<CUtensorMap> maps;
+    const int nvec = krydim + 4;
+    for (auto &c : bp.classes) {
+        c.map_base = (int)maps.size();
+        if (!c.any_rows) continue;
+        for (int sl = 0; sl < c.nslots; sl++)
+            for (int v = 0; v < nvec; v++)
+                maps.push_back(make_row_map(static_cast<char *>(bp.ws) + (size_t)sl * c.ws_stride +
+                                                (size_t)v * c.vec_stride,
+                                            c.maxlen, 1));
+    }
+    if (!maps.empty()) {
+        RP_CUDA(cudaMalloc((void **)&bp.maps, maps.size() * sizeof(CUtensorMap)));
+        RP_CUDA(cudaMemcpy(bp.maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                           cudaMemcpyHostToDevice));
     }
     RP_CUDA(cudaMalloc((void **)&bp.err, sizeof(unsigned)));
     RP_CUDA(cudaMemset(bp.err, 0, sizeof(unsigned)));
@@ -714,6 +948,10 @@ static BatchArgs class_args(const BatchPlan &bp, const BatchClass &c, int ntimes
     a.ws_stride = c.ws_stride;
     a.vec_stride = c.vec_stride;
     a.err = bp.err;
+    a.maps = c.any_rows ? bp.maps + c.map_base : nullptr;
+    a.nvec = bp.krydim + 4;
+    a.stage_bytes = stage_bytes(c);
+    a.table_bytes = table_bytes(c);
     return a;
 }
 

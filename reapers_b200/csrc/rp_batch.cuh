@@ -13,7 +13,10 @@ struct alignas(16) BatchProblem {
     const TermDesc<float> *terms;   // grouped by x >> B (tiled-kernel records)
     const GroupDesc *groups;
     const Cplx<float> *psi0;        // initial state (device)
+    const RowTerm<float> *rterms;   // row-kernel records (rows != 0)
+    const RowGroup *rgroups;
     int len, B, ntiles, ngroups;
+    int rows, rnterms, rngroups, pad;   // H.psi by 2-D TMA row tiles when rows != 0
     uint32_t wx, wz, vx, vz;        // W and V Pauli strings (X, Z masks)
     float wcr, wci, vcr, vci;       // their coefficients
 };
@@ -22,7 +25,9 @@ struct alignas(16) BatchProblem {
 // (clusters of `team` CTAs) of which `nslots` are resident.
 struct BatchClass {
     int team = 1, first = 0, count = 0, nslots = 0, maxB = 8, maxlen = 0;
+    bool any_rows = false, any_tiled = false;
     size_t smem = 0, ws_stride = 0, vec_stride = 0;
+    int map_base = 0;                        // first TMA map of this class's slots
 };
 
 struct BatchPlan {
@@ -30,6 +35,8 @@ struct BatchPlan {
     double tol = 0;
     std::vector<BatchClass> classes;         // in launch order
     std::vector<ApplyPlan> plans;            // per problem (host tables + device copies)
+    std::vector<RowPlan> rplans;             // per problem: row-kernel tables (when used)
+    CUtensorMap *maps = nullptr;             // [class slots][vector] 2-D TMA maps of the workspaces
     std::vector<BatchProblem> probs;         // device-pointer records, by class, largest first
     std::vector<int> order;                  // probs[i] is problem order[i]
     BatchProblem *d_probs = nullptr;
@@ -45,8 +52,10 @@ struct BatchPlan {
 
 // Problem p: len[p] qubits, nterms[p] terms (bits, coeff as for rp_ham_create),
 // W and V single strings, psi0[p] a device complex64 vector, tile[p] the tile
-// exponent (8..11, 0 = default), team[p] the CTAs per problem (1, 2, 4, 8 or
-// 16; 0 = default); tile and team may be null.
+// exponent (8..11, 0 = default) of the bulk-copy tile loop, team[p] the CTAs
+// per problem (1, 2, 4, 8 or 16; 0 = default); tile and team may be null.
+// Tile 12 selects the row-tile loop (2-D TMA, 4096-element swizzled tiles)
+// for states of at least 2^12 elements.
 void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms,
                  const uint64_t *const *bits, const double *const *coeff, const uint64_t *wbits,
                  const double *wcoeff, const uint64_t *vbits, const double *vcoeff,

@@ -63,7 +63,7 @@ def test_batched_matches_single_problem_mixed_path(cuda):
 
 def test_batched_rejects_bad_tile(cuda):
     probs, _ = make_problems([(16, 4)])
-    probs[0]["tile"] = 12
+    probs[0]["tile"] = 13
     with pytest.raises(rb.RPError):
         rb.BatchOTOC(probs)
 
@@ -110,3 +110,23 @@ def test_batched_rejects_bad_team(cuda):
     probs[0]["team"] = 3
     with pytest.raises(rb.RPError):
         rb.BatchOTOC(probs)
+
+
+@pytest.mark.parametrize("team", [1, 4, 16])
+def test_batched_row_tiles_match_tile_loop(cuda, team):
+    """The row-tile H.psi loop (2-D TMA swizzled tiles, tile exponent 12)
+    against the bulk-copy tile loop (exponent 11) on the same problems."""
+    specs = [(24, 8), (28, 8), (32, 4)]
+    probs, refs = make_problems(specs, seed=31)
+    times = np.array([0.0, 0.9])
+    out = {}
+    for tile in (11, 12):
+        b = rb.BatchOTOC([dict(p, tile=tile, team=team) for p in probs], krydim=12, tol=1e-7,
+                         max_restarts=16)
+        out[tile] = b.run(times)
+        b.close()
+    assert np.abs(out[11][0] - out[12][0]).max() < 2e-6
+    assert np.abs(out[11][1] - out[12][1]).max() <= 12
+    for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
+        ref = O.otoc(L, bits, coeff, w, v, psi, times, 12, 1e-12)
+        assert np.abs(out[12][0][p] - ref).max() < 2e-5, (p, out[12][0][p], ref)
