@@ -445,30 +445,25 @@ def run_ours(args):
     alg_dram = info["alg_bytes_dram"]
     achieved_dram = alg_dram / t_step / 1e9
 
-    # end to end through the C ABI with host buffers: H2D of the state, apply,
-    # D2H of the result, every step
+    # end to end through the public API with host buffers: every step copies
+    # its input state from pinned host memory to the device, applies H and
+    # copies the result back (rp_apply_host: the copies of neighbouring steps
+    # overlap the product on separate streams)
     esize = 8 if cfg["dtype"] == "c64" else 16
     nbytes = (1 << L) * esize
     hx = torch.empty(1 << L, dtype=x.dtype, pin_memory=True)
-    hy = torch.empty_like(hx, pin_memory=True)
+    hy = [torch.empty_like(hx, pin_memory=True) for _ in range(2)]
     hx.copy_(x.cpu())
-    from reapers_b200 import _lib
-    import ctypes as C
-
-    def e2e_step():
-        _lib.call("rp_memcpy", C.c_void_p(x.data_ptr()), C.c_void_p(hx.data_ptr()), nbytes, 0)
-        ham.apply(y, x)
-        _lib.call("rp_memcpy", C.c_void_p(hy.data_ptr()), C.c_void_p(y.data_ptr()), nbytes, 1)
-
-    e2e_step()
+    del y
+    torch.cuda.empty_cache()
+    k2 = max(3, args.steps // 2)
+    ham.apply_host(hy[:1], [hx])   # warm-up (allocates the pipeline buffers)
     barrier()
     torch.cuda.synchronize()
-    k2 = max(3, args.steps // 2)
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(st)
-    for _ in range(k2):
-        e2e_step()
+    ham.apply_host([hy[i & 1] for i in range(k2)], [hx] * k2)
     f1.record(st)
     f1.synchronize()
     t_e2e = f0.elapsed_time(f1) / 1e3 / k2
@@ -477,6 +472,7 @@ def run_ours(args):
         tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_e2e = float(tt.item())
+    rb._lib.call("rp_workspace_release")
     e2e_value = alg * world / t_e2e / 1e9
 
     peak, peak_kind = measured_peak()
@@ -512,7 +508,7 @@ def run_ours(args):
         "clocks": clocks,
     }
     if args.config == "c4" and not args.no_otoc:
-        del x, y, ham
+        del x, ham
         torch.cuda.empty_cache()
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
     if args.config == "c4" and not args.no_batch:

@@ -141,6 +141,13 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info);
 /* GPUImpl::apply_ops (src/krnl.cu:220-257): out = H in, or out += H in when
  * accumulate != 0.  in and out must differ. */
 int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
+/* out_host[i] = H in_host[i] for i < n: n states in HOST memory (2^len
+ * elements of the Hamiltonian's precision each; pinned memory lets the
+ * copies run asynchronously).  Pipelined over two device buffer pairs kept by
+ * the library: the copy of state i+1 to the device and of result i-1 to the
+ * host overlap H.psi on state i.  Returns when every result is on the host.
+ * No reference counterpart: the reference applies one resident state. */
+int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *out_host);
 
 /* Krylov<Impl>::evolve (inc/algo.h:267-365) as called by State::evolve
  * (inc/state.h:415-424): psi <- exp(-(beta + i t) H) psi in place, restarted
@@ -150,7 +157,8 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
 int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double tol,
               int max_iters, rp_evolve_stats_t *stats);
 
-/* Free the cached Krylov workspace (krydim + 2 vectors). */
+/* Free the cached Krylov workspace (krydim + 2 vectors) and the device
+ * buffers of rp_apply_host. */
 int rp_workspace_release(void);
 
 /* --- time-stepped Krylov primitives (no reference counterpart: the

@@ -106,6 +106,22 @@ class Hamiltonian:
         _lib.call("rp_apply", self._h, _ptr(out), _ptr(inp), 1 if accumulate else 0)
         return out
 
+    def apply_host(self, outs, ins):
+        """outs[i] = H ins[i] for CPU tensors (pinned for overlap): one call,
+        the host<->device copies pipelined with the products (rp_apply_host)."""
+        n = len(ins)
+        if len(outs) != n:
+            raise ValueError("outs and ins differ in length")
+        want = 1 << self.len
+        for t in list(ins) + list(outs):
+            if t.is_cuda or not t.is_contiguous() or t.numel() != want or _tcode(t) != self.dtype:
+                raise ValueError("host vectors must be contiguous CPU tensors of the "
+                                 "Hamiltonian's size and precision")
+        ip = (C.c_void_p * n)(*[t.data_ptr() for t in ins])
+        op = (C.c_void_p * n)(*[t.data_ptr() for t in outs])
+        _lib.call("rp_apply_host", self._h, n, ip, op)
+        return outs
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().rp_ham_destroy(self._h)

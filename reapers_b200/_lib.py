@@ -73,6 +73,7 @@ _SIGS = {
     "rp_ham_destroy": (C.c_int, [_VP]),
     "rp_ham_info": (C.c_int, [_VP, C.POINTER(HamInfo)]),
     "rp_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "rp_apply_host": (C.c_int, [_VP, C.c_int, C.POINTER(_VP), C.POINTER(_VP)]),
     "rp_evolve": (C.c_int, [_VP, _VP, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                             C.POINTER(EvolveStats)]),
     "rp_workspace_release": (C.c_int, []),

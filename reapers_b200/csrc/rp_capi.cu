@@ -102,10 +102,13 @@ int rp_init(int device) {
     }
 }
 
+static void pipe_release();
+
 int rp_shutdown(void) {
     try {
         std::lock_guard<std::mutex> lk(g_mu);
         workspace_release(g_ws);
+        pipe_release();
         if (g_stream) cudaStreamDestroy(g_stream);
         g_stream = nullptr;
         return RP_OK;
@@ -344,6 +347,87 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate) {
     });
 }
 
+// Device buffers and streams of rp_apply_host, kept between calls.
+struct HostPipe {
+    size_t bytes = 0;
+    void *din[2] = {nullptr, nullptr}, *dout[2] = {nullptr, nullptr};
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t in_ready[2] = {}, comp_done[2] = {}, out_done[2] = {};
+};
+static HostPipe g_pipe;
+
+static void pipe_release() {
+    HostPipe &p = g_pipe;
+    for (int b = 0; b < 2; b++) {
+        if (p.din[b]) cudaFree(p.din[b]);
+        if (p.dout[b]) cudaFree(p.dout[b]);
+        if (p.in_ready[b]) cudaEventDestroy(p.in_ready[b]);
+        if (p.comp_done[b]) cudaEventDestroy(p.comp_done[b]);
+        if (p.out_done[b]) cudaEventDestroy(p.out_done[b]);
+    }
+    if (p.s_in) cudaStreamDestroy(p.s_in);
+    if (p.s_out) cudaStreamDestroy(p.s_out);
+    p = HostPipe{};
+}
+
+static void pipe_ensure(size_t bytes) {
+    HostPipe &p = g_pipe;
+    if (!p.s_in) {
+        RP_CUDA(cudaStreamCreateWithFlags(&p.s_in, cudaStreamNonBlocking));
+        RP_CUDA(cudaStreamCreateWithFlags(&p.s_out, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; b++) {
+            RP_CUDA(cudaEventCreateWithFlags(&p.in_ready[b], cudaEventDisableTiming));
+            RP_CUDA(cudaEventCreateWithFlags(&p.comp_done[b], cudaEventDisableTiming));
+            RP_CUDA(cudaEventCreateWithFlags(&p.out_done[b], cudaEventDisableTiming));
+        }
+    }
+    if (p.bytes >= bytes) return;
+    for (int b = 0; b < 2; b++) {
+        if (p.din[b]) cudaFree(p.din[b]);
+        if (p.dout[b]) cudaFree(p.dout[b]);
+        p.din[b] = p.dout[b] = nullptr;
+    }
+    p.bytes = 0;
+    for (int b = 0; b < 2; b++) {
+        if (cudaMalloc(&p.din[b], bytes) != cudaSuccess || cudaMalloc(&p.dout[b], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{RP_E_NOMEM, "failed to allocate the host-apply device buffers"};
+        }
+    }
+    p.bytes = bytes;
+}
+
+int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *out_host) {
+    return guarded([&] {
+        RP_REQUIRE(h && n >= 0 && (n == 0 || (in_host && out_host)), RP_E_INVALID, "bad argument");
+        if (n == 0) return;
+        const size_t bytes = (size_t)esize(h->plan.dtype) << h->plan.len;
+        pipe_ensure(bytes);
+        HostPipe &p = g_pipe;
+        for (int i = 0; i < n; i++) {
+            RP_REQUIRE(in_host[i] && out_host[i], RP_E_INVALID, "null host vector");
+            const int b = i & 1;
+            // buffer b is free once H.psi i-2 has read it
+            if (i >= 2) RP_CUDA(cudaStreamWaitEvent(p.s_in, p.comp_done[b], 0));
+            RP_CUDA(cudaMemcpyAsync(p.din[b], in_host[i], bytes, cudaMemcpyHostToDevice, p.s_in));
+            RP_CUDA(cudaEventRecord(p.in_ready[b], p.s_in));
+            RP_CUDA(cudaStreamWaitEvent(g_stream, p.in_ready[b], 0));
+            // the result buffer b is free once result i-2 reached the host
+            if (i >= 2) RP_CUDA(cudaStreamWaitEvent(g_stream, p.out_done[b], 0));
+            ApplyLaunch L;
+            L.in = p.din[b];
+            L.out = p.dout[b];
+            apply_launch(h->plan, L, g_stream);
+            RP_CUDA(cudaEventRecord(p.comp_done[b], g_stream));
+            RP_CUDA(cudaStreamWaitEvent(p.s_out, p.comp_done[b], 0));
+            RP_CUDA(cudaMemcpyAsync(out_host[i], p.dout[b], bytes, cudaMemcpyDeviceToHost, p.s_out));
+            RP_CUDA(cudaEventRecord(p.out_done[b], p.s_out));
+        }
+        RP_CUDA(cudaStreamSynchronize(p.s_out));
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+    });
+}
+
 int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double tol,
               int max_iters, rp_evolve_stats_t *stats) {
     return guarded([&] {
@@ -518,6 +602,7 @@ int rp_workspace_release(void) {
     return guarded([&] {
         RP_CUDA(cudaStreamSynchronize(g_stream));
         workspace_release(g_ws);
+        pipe_release();
     });
 }
 

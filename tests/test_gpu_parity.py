@@ -248,3 +248,24 @@ def test_ground_state_lanczos_matches_dense(model):
     gv = g.cpu().numpy()
     assert np.linalg.norm(Hd @ gv - E0 * gv) <= 1e-6
     ham.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_apply_host_pipeline_matches_device_apply(dtype):
+    """rp_apply_host (host states, copies overlapped with the products) gives
+    the device apply's results for every state of the sequence."""
+    import reapers_b200 as rb
+    L = 19
+    bits, coeff = rb.syk.sparse_syk(2 * L, 8, seed=2)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    ins = [rb.random_state(L, dtype, seed=s).cpu().pin_memory() for s in range(5)]
+    outs = [torch.empty(1 << L, dtype=tdt).pin_memory() for _ in range(5)]
+    ham.apply_host(outs, ins)
+    ham.apply_host([], [])
+    for x, got in zip(ins, outs):
+        y = torch.empty(1 << L, dtype=tdt, device="cuda")
+        ham.apply(y, x.cuda())
+        assert torch.equal(got, y.cpu())
+    ham.close()
