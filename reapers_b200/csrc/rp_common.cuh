@@ -155,4 +155,25 @@ struct CompSum {
     __device__ __forceinline__ double value() const { return hi + lo; }
 };
 
+// Compensated sum of v[0], v[stride], ..., v[(n-1) stride] by one warp: lane
+// l sums the indices congruent to l mod 32, then the 32 (hi, lo) pairs meet
+// in a butterfly.  TwoSum's error term is exact whatever the operand order,
+// so every lane ends with the same bits and the result is the same run to run.
+__device__ __forceinline__ double warp_compsum(const double *v, int n, size_t stride) {
+    const int lane = threadIdx.x & 31;
+    CompSum c;
+    for (int g = lane; g < n; g += 32) c.add(v[(size_t)g * stride]);
+    double hi = c.hi, lo = c.lo;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ohi = __shfl_xor_sync(0xffffffffu, hi, o);
+        const double olo = __shfl_xor_sync(0xffffffffu, lo, o);
+        double sm, e;
+        two_sum(hi, ohi, sm, e);
+        hi = sm;
+        lo = (lo + olo) + e;
+    }
+    return hi + lo;
+}
+
 }  // namespace rp

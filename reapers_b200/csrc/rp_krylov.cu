@@ -145,19 +145,19 @@ __global__ void k_kry_begin(KryDev *s, int krydim, int restart) {
     for (int i = threadIdx.x; i < 2 * krydim * krydim; i += blockDim.x) s->H[i] = 0.0;
 }
 
-// h_i = sigma_i <u_i|w> for i <= j, reduced in fixed order from per-CTA partials.
+// h_i = sigma_i <u_i|w> for i <= j, reduced in a fixed order from per-CTA
+// partials, one warp per basis vector.
 __global__ void k_kry_proj(KryDev *s, const double *partials, int grid, int j, int pass) {
     if (!s->active) return;
     if (pass > 1 && !s->again) return;
     const int n = j + 1;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        CompSum re, im;
-        for (int g = 0; g < grid; g++) {
-            re.add(partials[((size_t)g * n + i) * 2 + 0]);
-            im.add(partials[((size_t)g * n + i) * 2 + 1]);
-        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < n; i += nw) {
+        const double re = warp_compsum(partials + (size_t)i * 2, grid, (size_t)n * 2);
+        const double im = warp_compsum(partials + (size_t)i * 2 + 1, grid, (size_t)n * 2);
+        if (lane != 0) continue;
         const double sg = s->sigma[i];
-        const double hr = sg * re.value(), hi = sg * im.value();
+        const double hr = sg * re, hi = sg * im;
         if (pass == 1) {
             s->hacc[2 * i] = hr;
             s->hacc[2 * i + 1] = hi;
@@ -175,12 +175,11 @@ __global__ void k_kry_proj(KryDev *s, const double *partials, int grid, int j, i
 // (inc/algo.h:86-106): continue while niter < 3, norm != 0 and
 // norm < eta * old_norm, old_norm starting at eta / 2.
 __global__ void k_kry_norm(KryDev *s, const double *np, int grid, int j, int krydim, int pass) {
-    if (threadIdx.x != 0) return;
     if (!s->active) return;
     if (pass > 1 && !s->again) return;
-    CompSum c;
-    for (int g = 0; g < grid; g++) c.add(np[g]);
-    const double norm = sqrt(c.value());
+    const double sq = warp_compsum(np, grid, 1);   // one warp
+    if (threadIdx.x != 0) return;
+    const double norm = sqrt(sq);
     const double eta = 1.0 / sqrt(2.0);
     const double old = pass == 1 ? eta / 2 : s->norm;
     s->old_norm = old;
@@ -340,13 +339,13 @@ void krylov_evolve(const ApplyPlan &plan, KryWorkspace &ws, void *psi, double t_
                 apply_launch(plan, L, st);
                 multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, nullptr, st);
             }
-            k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, agrid, j, 1);
+            k_kry_proj<<<1, 256, 0, st>>>(s, ws.partials, agrid, j, 1);
             multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials, &s->active,
                        nullptr, st);
             k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, krydim, 1);
             for (int pass = 2; pass <= 3; pass++) {
                 multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, &s->again, st);
-                k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, rgrid, j, pass);
+                k_kry_proj<<<1, 256, 0, st>>>(s, ws.partials, rgrid, j, pass);
                 multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials,
                            &s->active, &s->again, st);
                 k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, krydim, pass);
@@ -424,13 +423,13 @@ void krylov_arnoldi(const ApplyPlan &plan, KryWorkspace &ws, const void *psi, in
             apply_launch(plan, L, st);
             multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, nullptr, st);
         }
-        k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, agrid, j, 1);
+        k_kry_proj<<<1, 256, 0, st>>>(s, ws.partials, agrid, j, 1);
         multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials, &s->active,
                    nullptr, st);
         k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, m, 1);
         for (int pass = 2; pass <= 3; pass++) {
             multi_dot_partials(dtype, D, tab, j + 1, w, ws.partials, &s->active, &s->again, st);
-            k_kry_proj<<<1, 64, 0, st>>>(s, ws.partials, rgrid, j, pass);
+            k_kry_proj<<<1, 256, 0, st>>>(s, ws.partials, rgrid, j, pass);
             multi_axpy(dtype, D, tab, j + 1, nullptr, s->coef, w, ws.norm_partials, &s->active,
                        &s->again, st);
             k_kry_norm<<<1, 32, 0, st>>>(s, ws.norm_partials, rgrid, j, m, pass);

@@ -129,11 +129,22 @@ __global__ void __launch_bounds__(HID) k_mlp_grad(MlpDims d, const float *params
     }
 }
 
-__global__ void k_mlp_reduce(int np, int nparts, const float *gpart, float scale, float *g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int p = 0; p < nparts; p++) s += gpart[(size_t)p * np + i];
-        g[i] = (float)(s * scale);
+// g = scale * sum of the per-CTA partials: a block of 32 parameters x 8
+// warps, warp y taking partials y, y + 8, ..., then the 8 sums in order.
+__global__ void __launch_bounds__(256) k_mlp_reduce(int np, int nparts, const float *gpart,
+                                                    float scale, float *g) {
+    __shared__ double red[8][33];
+    const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + x;
+    double sum = 0.0;
+    if (i < np)
+        for (int p = y; p < nparts; p += 8) sum += gpart[(size_t)p * np + i];
+    red[y][x] = sum;
+    __syncthreads();
+    if (y == 0 && i < np) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += red[w][x];
+        g[i] = (float)(t * scale);
     }
 }
 
@@ -235,7 +246,7 @@ static float grad_device(Mlp &net, const float *dX, const float *dY, int n, floa
     const int nparts = (n + per - 1) / per;
     k_mlp_grad<<<nparts, HID, grad_smem(d), st>>>(d, net.params, dX, dY, n, per, gpart, lpart);
     RP_CUDA(cudaGetLastError());
-    k_mlp_reduce<<<(d.np + 255) / 256, 256, 0, st>>>(d.np, nparts, gpart, 1.f / n, net.g);
+    k_mlp_reduce<<<(d.np + 31) / 32, 256, 0, st>>>(d.np, nparts, gpart, 1.f / n, net.g);
     RP_CUDA(cudaGetLastError());
     std::vector<float> lp(nparts);
     RP_CUDA(cudaMemcpyAsync(lp.data(), lpart, nparts * sizeof(float), cudaMemcpyDeviceToHost, st));
