@@ -195,6 +195,63 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
     return out
 
 
+def evolve_leg_c2(seed=0, t=10.0, krydim=30, cpu=True):
+    """C2: exp(-iHt) psi for sparse SYK N = 48 (24 qubits, k = 8, 384 terms),
+    one random state, m = 30, t = 10: the plain FP64 path (tol = FP64
+    epsilon, the reference's default) against the mixed path (FP32 vectors
+    and H.psi, FP64 inner products / Hessenberg / expm, tol = FP32 epsilon);
+    error = ||psi_mixed - psi_fp64|| / ||psi_fp64||.  The reference CPU
+    evolve is estimated from a timed sample of its H.psi (2^18 of 2^24
+    output rows, all host threads) times the FP64 H.psi count -- a lower
+    bound (its orthogonalisation is not counted), labelled as such."""
+    import torch
+    import reapers_b200 as rb
+    cfg = CONFIGS["c2"]
+    N, L = cfg["N"], cfg["N"] // 2
+    bits, coeff = rb.syk.sparse_syk(N, k=cfg["k"], seed=seed + 2000)
+    psi64 = rb.random_state(L, "c128", seed=seed + 3, normalize=True)
+    out = {"workload": f"exp(-iHt) psi, sparse SYK N={N} (2^{L}), k={cfg['k']}, t={t}, m={krydim}"}
+    res = {}
+    for name, dt, tol in (("fp64_plain", "c128", float(np.finfo(np.float64).eps)),
+                          ("mixed_fp32", "c64", float(np.finfo(np.float32).eps))):
+        ham = rb.Hamiltonian(L, bits, coeff, dt)
+        x = psi64.clone() if dt == "c128" else torch.empty(1 << L, dtype=torch.complex64,
+                                                           device="cuda")
+        if dt == "c64":
+            rb.copy(x, psi64)
+        rb.evolve(ham, x.clone(), 0.05, 0.0, krydim, tol)   # warm-up (workspace, plan)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = rb.evolve(ham, x, t, 0.0, krydim, tol)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        res[name] = x.to(torch.complex128)
+        out[name] = {"seconds": round(el, 4), "applies": st["applies"],
+                     "restarts": st["restarts"], "tol": tol}
+        ham.close()
+        rb._lib.call("rp_workspace_release")
+        torch.cuda.empty_cache()
+    err = (torch.linalg.vector_norm(res["mixed_fp32"] - res["fp64_plain"]) /
+           torch.linalg.vector_norm(res["fp64_plain"])).item()
+    out["mixed_rel_err_vs_fp64"] = err
+    out["speedup_mixed_vs_fp64"] = round(out["fp64_plain"]["seconds"] /
+                                         out["mixed_fp32"]["seconds"], 3)
+    if cpu:
+        try:
+            rows = 1 << 18
+            cb = cpu_reference(cfg, bits, coeff, 0.0, rows, 1)
+            per_apply = cb["seconds"] * ((1 << L) / rows)
+            est = per_apply * out["fp64_plain"]["applies"]
+            out["cpu_reference_estimate"] = {
+                "seconds_lower_bound": round(est, 2), "cores": cb["threads"],
+                "sample": f"reference SpinOp::apply over {rows} of 2^{L} rows: "
+                          f"{per_apply:.3f} s per H.psi x {out['fp64_plain']['applies']} H.psi"}
+            out["speedup_fp64_vs_cpu_estimate"] = round(est / out["fp64_plain"]["seconds"], 1)
+        except Exception as e:   # a reported baseline only
+            out["cpu_reference_estimate"] = {"failed": str(e)}
+    return out
+
+
 def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
               seq_per_size=2, tune=True):
     """C3 sample: batched OTOC of nreal disorder realisations x nstates random
@@ -511,6 +568,8 @@ def run_ours(args):
         del x, ham
         torch.cuda.empty_cache()
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
+    if args.config == "c4" and not args.no_evolve:
+        line["evolve_c2"] = evolve_leg_c2(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
     if args.config == "c4" and not args.no_batch:
         line["otoc_batched_c3"] = batch_leg(seed=rank)
     if args.config == "c4" and not args.no_steps:
@@ -592,6 +651,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched C3 OTOC leg")
+    ap.add_argument("--no-evolve", action="store_true", help="skip the C2 evolve leg")
     ap.add_argument("--no-steps", action="store_true",
                     help="skip the learned step-controller C5 leg")
     ap.add_argument("--otoc-points", type=int, default=2,
