@@ -303,3 +303,36 @@ def test_dense_path_matches_krylov_on_c1_shape():
     gv = g.cpu().numpy()
     assert np.linalg.norm(Hd @ gv - E0 * gv) <= 1e-9
     ham.close()
+
+
+@pytest.mark.gpu
+def test_new_entry_points_reject_bad_arguments():
+    """Invalid arguments come back as RPError (status codes), the library
+    stays usable."""
+    import ctypes as C
+    import reapers_b200 as rb
+    from reapers_b200 import _lib, stepper as SP
+    L = 10
+    bits, coeff = rb.syk.sparse_syk(20, 4, seed=1)
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    x = rb.random_state(L, "c128", seed=1)
+    with pytest.raises(rb.RPError):
+        SP.arnoldi(ham, x, 1)                 # m < 2
+    with pytest.raises(rb.RPError):
+        SP.arnoldi(ham, x, 65)                # m > 64
+    with pytest.raises(rb.RPError):
+        SP.expm_first_columns(np.eye(2000), [1.0])   # m > 1024
+    with pytest.raises(rb.RPError):
+        SP.Mlp(0, 2)                          # no inputs
+    with pytest.raises(rb.RPError):
+        SP.Mlp(4, 9)                          # more than 8 outputs
+    with pytest.raises(rb.RPError):
+        _lib.call("rp_apply_host", ham.handle, 1, None, None)
+    with pytest.raises(rb.RPError):
+        _lib.call("rp_arnoldi_combine", None, C.c_void_p(x.data_ptr()))
+    # still usable
+    y = torch.empty_like(x)
+    ham.apply(y, x)
+    b = SP.arnoldi(ham, x, 6)
+    assert b.m_eff == 6
+    ham.close()
