@@ -564,15 +564,18 @@ def run_ours(args):
                      "term_applications_per_s": info["nterms"] * (1 << L) / t_step},
         "clocks": clocks,
     }
-    if args.config == "c4" and not args.no_otoc:
+    # the single-GPU characterisation legs run only at N = 1 (under torchrun
+    # every rank would repeat them while all GPUs are held)
+    legs = world == 1
+    if legs and args.config == "c4" and not args.no_otoc:
         del x, ham
         torch.cuda.empty_cache()
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
-    if args.config == "c4" and not args.no_evolve:
+    if legs and args.config == "c4" and not args.no_evolve:
         line["evolve_c2"] = evolve_leg_c2(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
-    if args.config == "c4" and not args.no_batch:
+    if legs and args.config == "c4" and not args.no_batch:
         line["otoc_batched_c3"] = batch_leg(seed=rank)
-    if args.config == "c4" and not args.no_steps:
+    if legs and args.config == "c4" and not args.no_steps:
         line["learned_steps_c5"] = step_leg(seed=rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
