@@ -12,7 +12,8 @@ Two layers:
   file:line it follows.
 * ``_ref/ref_driver`` -- the reference library itself compiled from its own
   headers against ``eigen_shim`` (built only where the reference checkout is
-  present; the prebuilt binary travels with the repository).  ``RefDriver``
+  present; the built binary is kept out of version control and travels with
+  the working tree).  ``RefDriver``
   runs it through files.
 
 Parity of the restatement is pinned against the reference driver and against
