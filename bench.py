@@ -1,9 +1,9 @@
 #!/usr/bin/env python3
 """Benchmark of the REAPERS hot path on B200: Pauli-sum H.psi throughput.
 
-Workload (default, ``--config c4``): sparse SYK with N = 56 Majoranas on
+Workload (default, ``--config syk56``): sparse SYK with N = 56 Majoranas on
 28 qubits (state of 2^28 complex64 = 2 GiB), k = 8, i.e. 448 quartic terms,
-H.psi in FP32.  ``--config c2``: sparse SYK N = 48 (24 qubits), 384 terms, FP64.
+H.psi in FP32.  ``--config syk48``: sparse SYK N = 48 (24 qubits), 384 terms, FP64.
 
 A step is one H.psi product over the whole state.  The metric is H.psi HBM
 GB/s: the algorithmic bytes of one apply, (G + 1) * 2^L * sizeof(element)
@@ -39,9 +39,9 @@ sys.path.insert(0, ROOT)
 METRIC = ("H·psi HBM GB/s; N=56 SYK OTOC pts/s, mixed+batched vs FP64 on B200 @1e-6")
 
 CONFIGS = {
-    "c4": dict(N=56, k=8, dtype="c64", workload="sparse SYK N=56 (28 qubits, 2^28 complex64 = 2 GiB), "
+    "syk56": dict(N=56, k=8, dtype="c64", workload="sparse SYK N=56 (28 qubits, 2^28 complex64 = 2 GiB), "
                "k=8, 448 quartic terms, H.psi in FP32"),
-    "c2": dict(N=48, k=8, dtype="c128", workload="sparse SYK N=48 (24 qubits, 2^24 complex128 = 256 MiB), "
+    "syk48": dict(N=48, k=8, dtype="c128", workload="sparse SYK N=48 (24 qubits, 2^24 complex128 = 256 MiB), "
                "k=8, 384 quartic terms, H.psi in FP64"),
 }
 
@@ -55,7 +55,7 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-PROFILE_SUMMARY = {"c4": "k_apply_rows_sparse_syk_n56_fp32.md"}
+PROFILE_SUMMARY = {"syk56": "k_apply_rows_sparse_syk_n56_fp32.md"}
 
 
 def profile_traffic(cfg_name):
@@ -144,7 +144,7 @@ def on_chip_bound(info, L, cfg, t_step, clocks):
 def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
     """N = 56 OTOC F(t) = <psi0| W(t) V W(t) V |psi0> (W = b_{N-1}, V = b_{N-2},
     the operators of examples/simple-syk-krylov.cc) on a bounded sample of the
-    C4 time grid (t = 0 and the first `npts` points of 20 on [0, 15]), one
+    20-point time grid on [0, 15] (t = 0 and the first `npts` points), one
     disorder realisation x one state, m = 16, for the plain FP64 path
     (reference default tol = FP64 epsilon) and the mixed path (FP32 vectors
     and H.psi, FP64 inner products / Hessenberg / expm, tol = FP32 epsilon).
@@ -195,8 +195,8 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
     return out
 
 
-def evolve_leg_c2(seed=0, t=10.0, krydim=30, cpu=True):
-    """C2: exp(-iHt) psi for sparse SYK N = 48 (24 qubits, k = 8, 384 terms),
+def evolve_leg(seed=0, t=10.0, krydim=30, cpu=True):
+    """exp(-iHt) psi for sparse SYK N = 48 (24 qubits, k = 8, 384 terms),
     one random state, m = 30, t = 10: the plain FP64 path (tol = FP64
     epsilon, the reference's default) against the mixed path (FP32 vectors
     and H.psi, FP64 inner products / Hessenberg / expm, tol = FP32 epsilon);
@@ -206,7 +206,7 @@ def evolve_leg_c2(seed=0, t=10.0, krydim=30, cpu=True):
     bound (its orthogonalisation is not counted), labelled as such."""
     import torch
     import reapers_b200 as rb
-    cfg = CONFIGS["c2"]
+    cfg = CONFIGS["syk48"]
     N, L = cfg["N"], cfg["N"] // 2
     bits, coeff = rb.syk.sparse_syk(N, k=cfg["k"], seed=seed + 2000)
     psi64 = rb.random_state(L, "c128", seed=seed + 3, normalize=True)
@@ -254,7 +254,7 @@ def evolve_leg_c2(seed=0, t=10.0, krydim=30, cpu=True):
 
 def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
               seq_per_size=2, tune=True):
-    """C3 sample: batched OTOC of nreal disorder realisations x nstates random
+    """Batched OTOC sample: nreal disorder realisations x nstates random
     states, sparse SYK k = 8 with N cycling over `sizes` (16/18/20 qubits),
     t = the first `npts` non-zero points of 40 on [0, 20], m = krydim; one
     persistent launch per time step in a CUDA graph, tile exponents from the
@@ -327,7 +327,7 @@ def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40)
 
 
 def step_leg(T=10.0, tol=1e-8, seed=0):
-    """C5: learned (dt, m) step controller vs Expokit's plain step control at
+    """Learned (dt, m) step controller vs Expokit's plain step control at
     equal tolerance, on XXZ L=24 (J = Jz = 1, fields U[-W, W], W in {0.5, 3})
     and sparse SYK N=48 (k=8), FP64, exp(-iHT) psi with T = 10.  The network
     is the committed model (trained on the GPU on plain-method traces of
@@ -567,16 +567,16 @@ def run_ours(args):
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
-    if legs and args.config == "c4" and not args.no_otoc:
+    if legs and args.config == "syk56" and not args.no_otoc:
         del x, ham
         torch.cuda.empty_cache()
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
-    if legs and args.config == "c4" and not args.no_evolve:
-        line["evolve_c2"] = evolve_leg_c2(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
-    if legs and args.config == "c4" and not args.no_batch:
-        line["otoc_batched_c3"] = batch_leg(seed=rank)
-    if legs and args.config == "c4" and not args.no_steps:
-        line["learned_steps_c5"] = step_leg(seed=rank)
+    if legs and args.config == "syk56" and not args.no_evolve:
+        line["evolve_syk48"] = evolve_leg(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
+    if legs and args.config == "syk56" and not args.no_batch:
+        line["otoc_batched_syk32_40"] = batch_leg(seed=rank)
+    if legs and args.config == "syk56" and not args.no_steps:
+        line["learned_steps"] = step_leg(seed=rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
@@ -650,15 +650,15 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="c4")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="syk56")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batched C3 OTOC leg")
-    ap.add_argument("--no-evolve", action="store_true", help="skip the C2 evolve leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched OTOC leg (sparse SYK N = 32/36/40)")
+    ap.add_argument("--no-evolve", action="store_true", help="skip the N = 48 FP64 vs mixed evolve leg")
     ap.add_argument("--no-steps", action="store_true",
-                    help="skip the learned step-controller C5 leg")
+                    help="skip the learned step-controller leg")
     ap.add_argument("--otoc-points", type=int, default=2,
-                    help="non-zero time points of the C4 grid in the OTOC sample")
+                    help="non-zero time points of the 20-point grid on [0, 15] in the N = 56 OTOC sample")
     ap.add_argument("--profile", action="store_true",
                     help="run two applies and exit (for an ncu capture)")
     args = ap.parse_args()

@@ -8,7 +8,7 @@ program).  Run in a checkout where the reference is present:
 Fixtures (numpy .npz):
   majorana_N{N}.npz        reference Majorana strings b_0..b_{N-1}, N = 4..20
   syk_dense_N8_seed5.npz   SYK::gen_ham(std::mt19937(5)) term list, N = 8
-  c1_dense_syk_N24.npz     dense SYK N = 24 (12 qubits, 10626 terms) from
+  dense_syk_N24.npz     dense SYK N = 24 (12 qubits, 10626 terms) from
                            SYK::gen_ham(std::mt19937(1)), psi0, and
                            State::evolve results at t = 0.5, 2.5, 5.0 (m = 20,
                            tol = 1e-12) with the reference's call counts
@@ -40,7 +40,7 @@ def main():
     L, b, c = R.syk(8, 0.0, 1.0, 5)
     np.savez_compressed(os.path.join(HERE, "syk_dense_N8_seed5.npz"), bits=b, coeff=c, len=L)
 
-    # C1: dense SYK N = 24, reference generator
+    # dense SYK N = 24, reference generator
     L, b, c = R.syk(24, 0.0, 1.0, 1)
     rng = np.random.default_rng(2024)
     psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
@@ -52,7 +52,7 @@ def main():
         outs.append(o)
         applies.append(st["applies"])
         prods.append(st["prods"])
-    np.savez_compressed(os.path.join(HERE, "c1_dense_syk_N24.npz"), bits=b, coeff=c, len=L,
+    np.savez_compressed(os.path.join(HERE, "dense_syk_N24.npz"), bits=b, coeff=c, len=L,
                         psi0=psi, times=np.array(times), out=np.array(outs),
                         applies=np.array(applies), prods=np.array(prods), krydim=20, tol=1e-12)
 

@@ -31,10 +31,10 @@ def test_apply_reference_fixture(cuda):
     assert np.linalg.norm(o - g["out"]) / np.linalg.norm(g["out"]) < 1e-13
 
 
-def test_c1_dense_syk_evolve_reference_fixture(cuda):
-    """C1: dense SYK N = 24 (12 qubits, all 10626 quartets from the
+def test_dense_syk_n24_evolve_reference_fixture(cuda):
+    """Dense SYK N = 24 (12 qubits, all 10626 quartets from the
     reference's SYK::gen_ham), m = 20, tol 1e-12, t = 0.5, 2.5, 5.0."""
-    g = gold("c1_dense_syk_N24.npz")
+    g = gold("dense_syk_N24.npz")
     L = int(g["len"])
     ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
     for k, t in enumerate(g["times"]):

@@ -272,7 +272,7 @@ def test_apply_host_pipeline_matches_device_apply(dtype):
 
 
 @pytest.mark.gpu
-def test_dense_path_matches_krylov_on_c1_shape():
+def test_dense_path_matches_krylov_on_dense_syk_n24():
     """Exact diagonalisation (inc/algo.h:27-54) on the GPU for the dense SYK
     of 12 qubits (all 10626 quartets of N = 24): the matrix equals the
     oracle's, exp(-iHt) psi equals the oracle's restarted Krylov at

@@ -140,8 +140,8 @@ def test_apply_matches_reference():
     assert np.abs(g["rt_coeff"] - g["coeff"]).max() == 0
 
 
-def test_c1_evolve_matches_reference():
-    g = gold("c1_dense_syk_N24.npz")
+def test_dense_syk_n24_evolve_matches_reference():
+    g = gold("dense_syk_N24.npz")
     L = int(g["len"])
     for k, t in enumerate(g["times"]):
         o, st = O.evolve(L, g["bits"], g["coeff"], g["psi0"], t, 0.0, int(g["krydim"]),
