@@ -157,8 +157,60 @@ int main(int argc, char **argv) {
     CSt ggh(gg);
     const double overlap = std::abs(gc * ggh);
 
+    // parity-block form (FermionOpBlockForm, BlockDiag, BlockState): the
+    // OTOC of examples/syk.cc (OTOC::evolve at beta = 0) on one block of
+    // N/2 - 1 qubits, and a BlockState evolved under BlockDiag(H_LL, H_RR)
+    SYK<double, CPUImpl, FermionOpBlockForm> bsyk_c(N, sp, 1.0);
+    SYK<double, B200Impl, FermionOpBlockForm> bsyk_g(N, sp, 1.0);
+    std::mt19937 brg_c(seed), brg_g(seed);
+    auto bham_c = bsyk_c.gen_ham(brg_c);
+    auto bham_g = bsyk_g.gen_ham(brg_g);
+    const double bterms = std::max(term_diff(bham_g.LL, bham_c.LL), term_diff(bham_g.RR, bham_c.RR));
+    CSt b0(L - 1);
+    {
+        std::mt19937 rs(seed + 2);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        for (size_t i = 0; i < b0.dim(); i++) b0[i] = complex<double>(nd(rs), nd(rs));
+        b0 *= 1.0 / b0.norm();
+    }
+    GSt bg0(b0);
+    const auto &opc = bsyk_c.fermion_ops(N - 2).LR;
+    const auto &opg = bsyk_g.fermion_ops(N - 2).LR;
+    CSt sc(b0);
+    GSt sg(bg0);
+    sc *= opc;
+    sg *= opg;
+    sc.evolve(bham_c.RR, t, 0.0, krydim, tol);
+    sg.evolve<B200Krylov>(bham_g.RR, t, 0.0, krydim, tol);
+    sc.evolve(bham_c.LL, -t, 0.0, krydim, tol);
+    sg.evolve<B200Krylov>(bham_g.LL, -t, 0.0, krydim, tol);
+    sc *= opc;
+    sg *= opg;
+    sc.evolve(bham_c.RR, t, 0.0, krydim, tol);
+    sg.evolve(bham_g.RR, t, 0.0, krydim, tol);   // the reference's Krylov on B200Impl
+    sc.evolve(bham_c.LL, -t, 0.0, krydim, tol);
+    sg.evolve(bham_g.LL, -t, 0.0, krydim, tol);
+    const auto Fbc = b0 * sc;
+    const auto Fbg = bg0 * sg;
+    const double otoc_block = std::abs(Fbg - Fbc) / std::abs(b0 * b0);
+    BlockState<double, CPUImpl> bsc(L - 1);
+    BlockState<double, B200Impl> bsg(L - 1);
+    bsc.L = b0;
+    bsc.R = CSt(b0);
+    bsc.R *= complex<double>(0.6, -0.8);
+    bsg.L = bg0;
+    bsg.R = GSt(bg0);
+    bsg.R *= complex<double>(0.6, -0.8);
+    bsc.evolve(bham_c, t, 0.0, krydim, tol);
+    bsg.evolve(bham_g, t, 0.0, krydim, tol);
+    const double block_evolve = std::max(rel_diff(bsg.L, bsc.L), rel_diff(bsg.R, bsc.R));
+
     std::printf(
-        "{\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
+        "{\"block_terms\": %.3e, \"otoc_block\": %.3e, \"F_block\": [%.12e, %.12e], "
+        "\"block_evolve\": %.3e, ", bterms, otoc_block, (double)Fbc.real(), (double)Fbc.imag(),
+        block_evolve);
+    std::printf(
+        "\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
         "\"apply\": %.3e, \"evolve_ref_krylov\": %.3e, \"evolve_b200krylov\": %.3e, "
         "\"evolve_beta\": %.3e, \"otoc\": %.3e, \"F\": [%.12e, %.12e], \"mutate\": %.3e, "
         "\"E0_cpu\": %.15e, \"E0_b200\": %.15e, \"ground_overlap\": %.15f}\n",

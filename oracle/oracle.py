@@ -256,6 +256,32 @@ class RefDriver:
         self._run("majorana", N, p)
         return read_terms(p)
 
+    def majorana_block(self, N):
+        """Parity-block Majoranas: (len, bits, coeff) with records LR_0, RL_0, LR_1, ..."""
+        p = os.path.join(self.tmp, "majb.terms")
+        self._run("majorana_block", N, p)
+        return read_terms(p)
+
+    def syk_block(self, N, sp, J, seed):
+        """SYK::gen_ham(mt19937(seed)) in parity-block form: (LL terms, RR terms)."""
+        a, b = os.path.join(self.tmp, "ll.terms"), os.path.join(self.tmp, "rr.terms")
+        self._run("syk_block", N, sp, J, seed, a, b)
+        return read_terms(a), read_terms(b)
+
+    def otoc_block(self, length, LL, RR, op, psi0, times, krydim, tol):
+        """examples/syk.cc's OTOC::evolve sequence at beta = 0 on one parity block."""
+        fl, fr, fo = (os.path.join(self.tmp, n) for n in ("ob_ll", "ob_rr", "ob_op"))
+        fv, fout = os.path.join(self.tmp, "ob_v"), os.path.join(self.tmp, "ob_out")
+        write_terms(fl, length, *LL)
+        write_terms(fr, length, *RR)
+        write_terms(fo, length, *op)
+        write_vec(fv, psi0)
+        self._run("otoc_block", fl, fr, fo, fv, fout, krydim, tol, *times)
+        with open(fout, "rb") as f:
+            n = int(np.frombuffer(f.read(8), np.int64)[0])
+            v = np.frombuffer(f.read(16 * n), np.float64)
+        return v[0::2] + 1j * v[1::2]
+
     def roundtrip(self, length, bits, coeff):
         p, q = os.path.join(self.tmp, "rt.in"), os.path.join(self.tmp, "rt.out")
         write_terms(p, length, bits, coeff)

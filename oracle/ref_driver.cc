@@ -212,6 +212,66 @@ int main(int argc, char **argv) {
         for (int n = 0; n < N; n++) write_records(f, Ops(syk.fermion_ops(n)));
         return 0;
     }
+    if (mode == "majorana_block") {
+        // majorana_block N out -- the parity-block Majoranas b_n = [[0, LR], [RL, 0]]
+        // of FermionOpBlockForm (inc/fermions.h:308-366) on N/2-1 qubits:
+        // records LR_0, RL_0, LR_1, RL_1, ...
+        int N = atoi(argv[2]);
+        SYK<double, CPUImpl, FermionOpBlockForm> syk(N, 0.0, 1.0);
+        std::ofstream f(argv[3], std::ios::binary);
+        int64_t T = 2 * N; int32_t l = N / 2 - 1;
+        f.write((const char *)&T, 8); f.write((const char *)&l, 4);
+        for (int n = 0; n < N; n++) {
+            write_records(f, Ops(syk.fermion_ops(n).LR));
+            write_records(f, Ops(syk.fermion_ops(n).RL));
+        }
+        return 0;
+    }
+    if (mode == "syk_block") {
+        // syk_block N sp J seed outLL outRR -- SYK::gen_ham with std::mt19937(seed)
+        // in parity-block form: the blocks H_LL and H_RR on N/2-1 qubits
+        int N = atoi(argv[2]); double sp = atof(argv[3]), J = atof(argv[4]);
+        unsigned seed = (unsigned)strtoul(argv[5], 0, 10);
+        std::mt19937 rg(seed);
+        SYK<double, CPUImpl, FermionOpBlockForm> syk(N, sp, J);
+        auto ham = syk.gen_ham(rg);
+        write_terms(argv[6], Ops(ham.LL), N / 2 - 1);
+        write_terms(argv[7], Ops(ham.RR), N / 2 - 1);
+        return 0;
+    }
+    if (mode == "otoc_block") {
+        // otoc_block termsLL termsRR opterm psi0 out krydim tol t1 t2 ...
+        //   OTOC::evolve of examples/syk.cc:270-283 at beta = 0 on one parity
+        //   block: s = op s; e^{-iH_RR t}; e^{+iH_LL t}; op; e^{-iH_RR t};
+        //   e^{+iH_LL t}; F = <psi0|s>
+        int len, lo;
+        auto LL = build_ops(read_terms(argv[2], len));
+        auto RR = build_ops(read_terms(argv[3], len));
+        auto op = build_ops(read_terms(argv[4], lo));
+        auto v = read_vec(argv[5]);
+        int krydim = atoi(argv[7]);
+        double tol = atof(argv[8]);
+        St init(len), s(len);
+        load_state(init, v);
+        std::ofstream f(argv[6], std::ios::binary);
+        int64_t npts = argc - 9;
+        f.write((const char *)&npts, 8);
+        for (int a = 9; a < argc; a++) {
+            double t = atof(argv[a]);
+            s = init;
+            s *= op;
+            s.evolve(RR, t, 0.0, krydim, tol);
+            s.evolve(LL, -t, 0.0, krydim, tol);
+            s *= op;
+            s.evolve(RR, t, 0.0, krydim, tol);
+            s.evolve(LL, -t, 0.0, krydim, tol);
+            auto c = init * s;
+            double re = c.real(), im = c.imag();
+            f.write((const char *)&re, 8);
+            f.write((const char *)&im, 8);
+        }
+        return 0;
+    }
     if (mode == "roundtrip") {
         // roundtrip terms out -- terms through SpinOp/HostSumOps and back
         int len; auto terms = read_terms(argv[2], len);

@@ -19,7 +19,7 @@ from . import syk  # noqa: F401  (term generators)
 
 __all__ = ["Hamiltonian", "evolve", "ground_state", "dot", "norm", "axpy", "scale", "random_state",
            "stream", "synchronize", "RPError", "RP_C64", "RP_C128", "dtype_code", "syk",
-           "otoc"]
+           "otoc", "otoc_block"]
 
 
 def dtype_code(dtype):
@@ -310,6 +310,27 @@ class BatchOTOC:
             self.close()
         except Exception:
             pass
+
+
+def otoc_block(ham_ll, ham_rr, op, psi0, times, krydim=5, tol=None):
+    """The parity-block OTOC of examples/syk.cc (OTOC::evolve, lines 270-283)
+    at beta = 0 on one block of N/2 - 1 qubits: s = op psi0; e^{-iH_RR t};
+    e^{+iH_LL t}; op; e^{-iH_RR t}; e^{+iH_LL t}; F(t) = <psi0|s>, with op a
+    Hamiltonian holding the LR block of the perturbing Majorana (b_{N-2} in
+    the example).  Returns (F values, H.psi count of the evolves)."""
+    import torch
+    vals, applies = [], 0
+    a = torch.empty_like(psi0)
+    b = torch.empty_like(psi0)
+    for t in times:
+        op.apply(a, psi0)
+        applies += evolve(ham_rr, a, t, 0.0, krydim, tol)["applies"]
+        applies += evolve(ham_ll, a, -t, 0.0, krydim, tol)["applies"]
+        op.apply(b, a)
+        applies += evolve(ham_rr, b, t, 0.0, krydim, tol)["applies"]
+        applies += evolve(ham_ll, b, -t, 0.0, krydim, tol)["applies"]
+        vals.append(dot(psi0, b))
+    return np.array(vals), applies
 
 
 def otoc(ham, w, v, psi0, times, krydim=5, tol=None):

@@ -127,16 +127,80 @@ def dense_syk(N, seed=0, J=1.0):
     return quartic_terms(N, q, Jq)
 
 
-def sparse_syk(N, k=8, seed=0, J=1.0):
-    """Sparse SYK with exactly k*N quartets drawn uniformly without replacement,
-    kept in gen_ham's loop order, couplings N(0,1) * scale of SYK(N, k, J)."""
+def sparse_syk_couplings(N, k=8, seed=0, J=1.0):
+    """(quartets, couplings) of the sparse SYK model below."""
     rng = np.random.default_rng(seed)
     total = math.comb(N, 4)
     T = int(round(k * N))
     ranks = np.sort(rng.choice(total, size=T, replace=False))
     q = _unrank_quartets(N, ranks)
     Jq = rng.standard_normal(T) * syk_scale(N, k, J)
-    return quartic_terms(N, q, Jq)
+    return q, Jq
+
+
+def sparse_syk(N, k=8, seed=0, J=1.0):
+    """Sparse SYK with exactly k*N quartets drawn uniformly without replacement,
+    kept in gen_ham's loop order, couplings N(0,1) * scale of SYK(N, k, J)."""
+    return quartic_terms(N, *sparse_syk_couplings(N, k, seed, J))
+
+
+def sparse_syk_block(N, k=8, seed=0, J=1.0):
+    """The same model (same quartets and couplings) in parity-block form:
+    ((H_LL bits, coeff), (H_RR bits, coeff)) on N/2 - 1 qubits."""
+    return quartic_terms_block(N, *sparse_syk_couplings(N, k, seed, J))
+
+
+def majorana_block(N, n, standard_gamma=True):
+    """The n-th Majorana in parity-block form, b_n = [[0, LR], [RL, 0]] on
+    N/2 - 1 qubits (FermionOpBlockForm, inc/fermions.h:308-366): for
+    n <= N - 2, LR = RL = the n-th non-block Majorana of N - 2 fermions without
+    the 1/sqrt 2 (n = N - 2 gives sz(N/2 - 2)); for n = N - 1, LR = -i I and
+    RL = i I.  Returns ((LR bits, coeff), (RL bits, coeff)), / sqrt 2 when
+    standard_gamma."""
+    if N < 4 or N & 1 or not 0 <= n < N:
+        raise ValueError("need an even N >= 4 and 0 <= n < N")
+    if n == N - 1:
+        lr, rl = (np.uint64(0), -1j), (np.uint64(0), 1j)
+    else:
+        b, c = majorana(N - 2, n, standard_gamma=False)
+        lr = rl = (b, c)
+    f = 1.0 / math.sqrt(2.0) if standard_gamma else 1.0
+    return (np.uint64(lr[0]), complex(lr[1]) * f), (np.uint64(rl[0]), complex(rl[1]) * f)
+
+
+def _merge(bits, coeff):
+    """Sum the coefficients of equal strings, in order of first occurrence
+    (HostSumOps::operator+=, inc/cpuimpl.h:233-253)."""
+    order, acc = [], {}
+    for b, c in zip(np.asarray(bits, dtype=np.uint64).tolist(), np.asarray(coeff).tolist()):
+        if b in acc:
+            acc[b] += c
+        else:
+            acc[b] = c
+            order.append(b)
+    return np.array(order, np.uint64), np.array([acc[b] for b in order], np.complex128)
+
+
+def quartic_terms_block(N, quartets, couplings):
+    """Parity blocks of H = sum_q J_q b_i b_j b_k b_l (products left to right):
+    H_LL = sum J_q LR_i RL_j LR_k RL_l and H_RR = sum J_q RL_i LR_j RL_k LR_l,
+    each as (bits, coeff) on N/2 - 1 qubits with equal strings merged."""
+    q = np.asarray(quartets, dtype=np.int64).reshape(-1, 4)
+    blocks = [majorana_block(N, n) for n in range(N)]
+    lr_b = np.array([blocks[n][0][0] for n in range(N)], np.uint64)
+    lr_c = np.array([blocks[n][0][1] for n in range(N)])
+    rl_b = np.array([blocks[n][1][0] for n in range(N)], np.uint64)
+    rl_c = np.array([blocks[n][1][1] for n in range(N)])
+    J = np.asarray(couplings, dtype=np.float64).astype(np.complex128)
+    out = []
+    for first, second in (((lr_b, lr_c), (rl_b, rl_c)), ((rl_b, rl_c), (lr_b, lr_c))):
+        bits = np.zeros(len(q), np.uint64)
+        coeff = J.copy()
+        for f in range(4):
+            src = first if f % 2 == 0 else second
+            bits, coeff = mul(bits, coeff, src[0][q[:, f]], src[1][q[:, f]])
+        out.append(_merge(bits, coeff))
+    return out[0], out[1]
 
 
 def xxz_chain(L, Jz=1.0, fields=None, J=1.0, periodic=False):

@@ -18,6 +18,11 @@ Fixtures (numpy .npz):
   otoc_N16.npz             dense SYK N = 16 from gen_ham(mt19937(3)),
                            F(t) at t = 0, 0.5, 1, 2 in the order of
                            examples/simple-syk-krylov.cc (m = 10, tol 1e-12)
+  majorana_block_N{N}.npz  parity-block Majoranas (LR, RL records), N = 6..12
+  syk_block_N12.npz        dense SYK N = 12 from gen_ham(mt19937(3)) in both
+                           forms (full terms; H_LL, H_RR), and the parity-block
+                           OTOC of examples/syk.cc at t = 0, 0.4, 1.1 with
+                           op = LR of b_{N-2} (m = 10, tol 1e-12)
 """
 import os
 import sys
@@ -95,6 +100,25 @@ def main():
                         w_bits=w[0], w_coeff=w[1], v_bits=vv[0], v_coeff=vv[1], psi0=psi,
                         times=np.array(times), F=vals, krydim=10, tol=1e-12,
                         applies=st["applies"])
+    # parity-block form: Majorana blocks, block Hamiltonians and the block OTOC
+    for N in (6, 8, 10, 12):
+        L, b, c = R.majorana_block(N)
+        np.savez_compressed(os.path.join(HERE, f"majorana_block_N{N}.npz"), bits=b, coeff=c,
+                            len=L)
+    N = 12
+    Lf, bf, cf = R.syk(N, 0.0, 1.0, 3)
+    (Lb, llb, llc), (_, rrb, rrc) = R.syk_block(N, 0.0, 1.0, 3)
+    rng = np.random.default_rng(12)
+    psi = rng.standard_normal(1 << Lb) + 1j * rng.standard_normal(1 << Lb)
+    psi /= np.linalg.norm(psi)
+    (ob, oc), _ = S.majorana_block(N, N - 2)
+    times = [0.0, 0.4, 1.1]
+    F = R.otoc_block(Lb, (llb, llc), (rrb, rrc), (np.array([ob]), np.array([oc])), psi, times,
+                     10, 1e-12)
+    np.savez_compressed(os.path.join(HERE, "syk_block_N12.npz"), full_bits=bf, full_coeff=cf,
+                        ll_bits=llb, ll_coeff=llc, rr_bits=rrb, rr_coeff=rrc, len=Lb, psi0=psi,
+                        times=np.array(times), F=F, op_bits=np.array([ob]),
+                        op_coeff=np.array([oc]), krydim=10, tol=1e-12)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

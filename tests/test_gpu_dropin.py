@@ -10,7 +10,9 @@ GPU-resident Krylov selected as State::evolve<B200Krylov>, imaginary-time
 evolution, the OTOC sequence of examples/simple-syk-krylov.cc, an apply
 after the operator is changed (device table dropped and rebuilt), and the
 reference's ground-state Lanczos (energy; state overlap where the ground
-state is not degenerate).
+state is not degenerate); and the parity-block form (FermionOpBlockForm,
+BlockDiag, BlockState): block term lists, the OTOC sequence of
+examples/syk.cc on one block, a block state evolve.
 """
 import json
 import os
@@ -45,6 +47,10 @@ def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
     for k in ("apply", "evolve_ref_krylov", "evolve_b200krylov", "evolve_beta", "mutate"):
         assert d[k] <= 1e-12, (k, d)
     assert d["otoc"] <= 1e-11, d
+    # parity-block form: block gen_ham, the examples/syk.cc OTOC on one block,
+    # a BlockState evolved under BlockDiag(H_LL, H_RR)
+    assert d["block_terms"] == 0.0
+    assert d["otoc_block"] <= 1e-11 and d["block_evolve"] <= 1e-12, d
     # ground state (inc/algo.h:180-257) from different random starts
     assert abs(d["E0_b200"] - d["E0_cpu"]) <= 1e-10 * abs(d["E0_cpu"]), d
     if N % 8 == 0:   # no parity-sector degeneracy: the same state up to a phase

@@ -69,3 +69,19 @@ def test_otoc_reference_fixture(cuda):
     # the reference counts the four single-string products per point too
     # (State::operator*= goes through Impl::apply_ops)
     assert applies + 4 * len(g["times"]) == int(g["applies"])
+
+
+def test_parity_block_otoc_reference_fixture(cuda):
+    """The parity-block OTOC of examples/syk.cc (one block of N/2 - 1 = 5
+    qubits, dense SYK N = 12 from the reference's generator, op = LR block of
+    b_{N-2}) against the reference's own values (FP64, <= 1e-12)."""
+    import reapers_b200 as rb
+    g = np.load(os.path.join(GOLD, "syk_block_N12.npz"))
+    L = int(g["len"])
+    ll = rb.Hamiltonian(L, g["ll_bits"], g["ll_coeff"], "c128")
+    rr = rb.Hamiltonian(L, g["rr_bits"], g["rr_coeff"], "c128")
+    op = rb.Hamiltonian(L, g["op_bits"], g["op_coeff"], "c128")
+    psi0 = torch.from_numpy(g["psi0"]).cuda()
+    F, applies = rb.otoc_block(ll, rr, op, psi0, g["times"], int(g["krydim"]), float(g["tol"]))
+    assert np.abs(F - g["F"]).max() <= 1e-12 * abs(g["F"][0]), (F, g["F"])
+    assert applies > 0

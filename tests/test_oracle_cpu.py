@@ -180,3 +180,35 @@ def test_xxz_chain_terms():
     assert len(b) == 3 * 3 + 4
     M = O.dense_matrix(4, b, c)
     assert np.abs(M - M.conj().T).max() < TOL   # Hermitian
+
+
+# --- parity-block form (FermionOpBlockForm, inc/fermions.h:308-366) ---------
+@pytest.mark.parametrize("N", [6, 8, 10, 12])
+def test_block_majoranas_match_reference(N):
+    import reapers_b200.syk as S
+    g = gold(f"majorana_block_N{N}.npz")
+    for n in range(N):
+        (lb, lc), (rb_, rc) = S.majorana_block(N, n)
+        assert int(g["bits"][2 * n]) == int(lb) and int(g["bits"][2 * n + 1]) == int(rb_)
+        assert abs(g["coeff"][2 * n] - lc) < 1e-15 and abs(g["coeff"][2 * n + 1] - rc) < 1e-15
+
+
+def test_block_hamiltonian_matches_reference_and_spectrum():
+    """The block form built from the reference's couplings (recovered from its
+    full-form terms) equals the reference's block gen_ham, and H_LL + H_RR
+    has the spectrum of the full Hamiltonian."""
+    import reapers_b200.syk as S
+    g = gold("syk_block_N12.npz")
+    N = 12
+    q = S.all_quartets(N)
+    ub, uc = S.quartic_terms(N, q, np.ones(len(q)))
+    assert np.array_equal(ub, g["full_bits"])
+    J = (g["full_coeff"] / uc).real
+    (llb, llc), (rrb, rrc) = S.quartic_terms_block(N, q, J)
+    assert np.array_equal(llb, g["ll_bits"]) and np.array_equal(rrb, g["rr_bits"])
+    assert np.abs(llc - g["ll_coeff"]).max() < 1e-15 and np.abs(rrc - g["rr_coeff"]).max() < 1e-15
+    Lb = int(g["len"])
+    ev_full = np.linalg.eigvalsh(O.dense_matrix(N // 2, g["full_bits"], g["full_coeff"]))
+    ev_blk = np.sort(np.concatenate([np.linalg.eigvalsh(O.dense_matrix(Lb, llb, llc)),
+                                     np.linalg.eigvalsh(O.dense_matrix(Lb, rrb, rrc))]))
+    np.testing.assert_allclose(ev_blk, ev_full, atol=1e-12)
