@@ -65,6 +65,9 @@ struct BatchArgs {
 struct BatchShared {
     double red[2 * BNW];
     double part[2][4];            // published partials: [buffer][re, im, ok, -]
+    double gpart[2][16];          // published grouped projections: [buffer][re, im x 8]
+    double gred[BNW][16];         // per-warp grouped sums
+    double gres[16];              // team totals of the grouped projections
     double sigma[BMAXK + 1];
     double hacc[2 * (BMAXK + 1)];
     double coef[2 * (BMAXK + 1)];
@@ -156,6 +159,62 @@ __device__ __noinline__ void team_dot(const Team &tm, const Cplx<float> *a, cons
     team_reduce(tm, sr, si, true, S);
     re = sr;
     im = si;
+}
+
+constexpr int TG = 8;   // basis vectors projected per pass over w
+
+// <u_i|w> for i in [i0, i0 + ng), ng <= TG, in one pass over w: per-thread
+// FP64 sums, fixed-order combination over the CTA's warps and then over the
+// team's CTAs (all CTAs hold the same bits).  One cluster barrier.
+__device__ __noinline__ void team_dots(const Team &tm, Cplx<float> *const *u, int i0, int ng,
+                                       const Cplx<float> *w, uint32_t n, BatchShared &S,
+                                       double *re, double *im) {
+    double sr[TG], si[TG];
+#pragma unroll
+    for (int q = 0; q < TG; q++) sr[q] = si[q] = 0.0;
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
+        const Cplx<float> y = w[k];
+#pragma unroll
+        for (int q = 0; q < TG; q++) {
+            if (q < ng) {
+                const Cplx<float> x = u[i0 + q][k];
+                sr[q] = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, sr[q]));
+                si[q] = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, si[q]));
+            }
+        }
+    }
+    // CTA: warp sums, then the warps in order
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < TG; q++) {
+        const double a = warp_sum(sr[q]), b = warp_sum(si[q]);
+        if (lane == 0) {
+            S.gred[warp][2 * q] = a;
+            S.gred[warp][2 * q + 1] = b;
+        }
+    }
+    __syncthreads();
+    const int buf = S.pbuf;
+    if (threadIdx.x < 2 * TG) {
+        CompSum c;
+        for (int wi = 0; wi < BNW; wi++) c.add(S.gred[wi][threadIdx.x]);
+        S.gpart[buf][threadIdx.x] = c.value();
+    }
+    team_sync();
+    cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x < 2 * ng) {
+        CompSum c;
+        for (unsigned r = 0; r < tm.size; r++) c.add(cl.map_shared_rank(&S.gpart[buf][0], r)[threadIdx.x]);
+        S.gres[threadIdx.x] = c.value();
+    }
+    __syncthreads();
+    for (int q = 0; q < ng; q++) {
+        re[q] = S.gres[2 * q];
+        im[q] = S.gres[2 * q + 1];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) S.pbuf = buf ^ 1;
+    __syncthreads();
 }
 
 // Element passes end with the generic-proxy writes fenced for the bulk
@@ -502,17 +561,20 @@ __device__ bool team_evolve(const Team &tm, const BatchProblem &P, Cplx<float> *
             int niter = 0;
             while (niter < 3 && norm != 0.0 && norm < eta * old) {
                 niter++;
-                for (int i = 0; i <= j; i++) {
-                    double hr, hi;
-                    team_dot(tm, S.u[i], w, n, S, hr, hi);
-                    const double sg = S.sigma[i];
-                    hr *= sg;
-                    hi *= sg;
+                for (int i0 = 0; i0 <= j; i0 += TG) {
+                    const int ng = j + 1 - i0 < TG ? j + 1 - i0 : TG;
+                    double hr[TG], hi[TG];
+                    team_dots(tm, S.u, i0, ng, w, n, S, hr, hi);
                     if (threadIdx.x == 0) {
-                        S.hacc[2 * i] = (niter == 1 ? 0.0 : S.hacc[2 * i]) + hr;
-                        S.hacc[2 * i + 1] = (niter == 1 ? 0.0 : S.hacc[2 * i + 1]) + hi;
-                        S.coef[2 * i] = -hr * sg;
-                        S.coef[2 * i + 1] = -hi * sg;
+                        for (int q = 0; q < ng; q++) {
+                            const int i = i0 + q;
+                            const double sg = S.sigma[i];
+                            const double r = hr[q] * sg, m_ = hi[q] * sg;
+                            S.hacc[2 * i] = (niter == 1 ? 0.0 : S.hacc[2 * i]) + r;
+                            S.hacc[2 * i + 1] = (niter == 1 ? 0.0 : S.hacc[2 * i + 1]) + m_;
+                            S.coef[2 * i] = -r * sg;
+                            S.coef[2 * i + 1] = -m_ * sg;
+                        }
                     }
                 }
                 __syncthreads();
