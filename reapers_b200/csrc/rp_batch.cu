@@ -60,6 +60,7 @@ struct BatchArgs {
     int nvec;                    // vectors per slot
     size_t stage_bytes;          // ring stages (a multiple of 1024)
     size_t table_bytes;          // row-kernel tables (0 without row-tile problems)
+    size_t rterm_bytes;          // the term table's share of table_bytes
 };
 
 struct BatchShared {
@@ -161,7 +162,45 @@ __device__ __noinline__ void team_dot(const Team &tm, const Cplx<float> *a, cons
     im = si;
 }
 
+// Basis-vector reads of the projection and update passes.  From 2^17
+// elements per state on they stream through L2 with evict-first priority
+// (ld.global.cs), which keeps the H.psi source tiles resident: measured
+// +7 % (18 qubits) and +5 % (20 qubits) batched OTOC throughput, while on
+// 16-qubit states, whose basis is re-read from L2, plain loads are 4.5 %
+// faster.  The choice is made once per pass (a template argument): a
+// run-time test inside the unrolled loads cost 15 % at every size.
+constexpr uint32_t STREAM_MIN = 1u << 17;
+template <bool STREAM>
+__device__ __forceinline__ Cplx<float> ld_basis(const Cplx<float> *p) {
+    if constexpr (STREAM) {
+        const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+        return Cplx<float>{v.x, v.y};
+    } else {
+        return *p;
+    }
+}
+
 constexpr int TG = 8;   // basis vectors projected per pass over w
+
+// This thread's FP64 partial sums of <u_i|w>, i in [i0, i0 + ng).
+template <bool STREAM>
+__device__ __forceinline__ void dots_pass(const Team &tm, Cplx<float> *const *u, int i0, int ng,
+                                          const Cplx<float> *w, uint32_t n, double (&sr)[TG],
+                                          double (&si)[TG]) {
+#pragma unroll
+    for (int q = 0; q < TG; q++) sr[q] = si[q] = 0.0;
+    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
+        const Cplx<float> y = w[k];
+#pragma unroll
+        for (int q = 0; q < TG; q++) {
+            if (q < ng) {
+                const Cplx<float> x = ld_basis<STREAM>(&u[i0 + q][k]);
+                sr[q] = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, sr[q]));
+                si[q] = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, si[q]));
+            }
+        }
+    }
+}
 
 // <u_i|w> for i in [i0, i0 + ng), ng <= TG, in one pass over w: per-thread
 // FP64 sums, fixed-order combination over the CTA's warps and then over the
@@ -170,23 +209,15 @@ __device__ __noinline__ void team_dots(const Team &tm, Cplx<float> *const *u, in
                                        const Cplx<float> *w, uint32_t n, BatchShared &S,
                                        double *re, double *im) {
     double sr[TG], si[TG];
-#pragma unroll
-    for (int q = 0; q < TG; q++) sr[q] = si[q] = 0.0;
-    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
-        const Cplx<float> y = w[k];
-#pragma unroll
-        for (int q = 0; q < TG; q++) {
-            if (q < ng) {
-                const Cplx<float> x = u[i0 + q][k];
-                sr[q] = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, sr[q]));
-                si[q] = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, si[q]));
-            }
-        }
-    }
+    if (n >= STREAM_MIN)
+        dots_pass<true>(tm, u, i0, ng, w, n, sr, si);
+    else
+        dots_pass<false>(tm, u, i0, ng, w, n, sr, si);
     // CTA: warp sums, then the warps in order
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int q = 0; q < TG; q++) {
+        if (q >= ng) break;
         const double a = warp_sum(sr[q]), b = warp_sum(si[q]);
         if (lane == 0) {
             S.gred[warp][2 * q] = a;
@@ -195,7 +226,7 @@ __device__ __noinline__ void team_dots(const Team &tm, Cplx<float> *const *u, in
     }
     __syncthreads();
     const int buf = S.pbuf;
-    if (threadIdx.x < 2 * TG) {
+    if (threadIdx.x < 2 * ng) {
         CompSum c;
         for (int wi = 0; wi < BNW; wi++) c.add(S.gred[wi][threadIdx.x]);
         S.gpart[buf][threadIdx.x] = c.value();
@@ -244,15 +275,16 @@ __device__ void team_string(const Team &tm, uint32_t x, uint32_t z, float cr, fl
     team_sync();
 }
 
-// w += sum_{i < nv} coef_i u_i over the team; returns ||w||^2 (team-wide).
-__device__ __noinline__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double *coef, int nv,
-                            Cplx<float> *w, uint32_t n, BatchShared &S) {
+// This thread's share of w += sum_{i < nv} coef_i u_i; returns its part of ||w||^2.
+template <bool STREAM>
+__device__ __forceinline__ double axpy_pass(const Team &tm, Cplx<float> *const *u, const double *coef,
+                                            int nv, Cplx<float> *w, uint32_t n) {
     double nrm = 0.0;
     for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
         const Cplx<float> w0 = w[k];
         double xr = w0.x, xi = w0.y;
         for (int i = 0; i < nv; i++) {
-            const Cplx<float> v = u[i][k];
+            const Cplx<float> v = ld_basis<STREAM>(&u[i][k]);
             const double cr = coef[2 * i], ci = coef[2 * i + 1];
             xr = fma(cr, (double)v.x, fma(-ci, (double)v.y, xr));
             xi = fma(cr, (double)v.y, fma(ci, (double)v.x, xi));
@@ -261,6 +293,14 @@ __device__ __noinline__ double team_axpy(const Team &tm, Cplx<float> *const *u, 
         w[k] = r;
         nrm = fma((double)r.x, (double)r.x, fma((double)r.y, (double)r.y, nrm));
     }
+    return nrm;
+}
+
+// w += sum_{i < nv} coef_i u_i over the team; returns ||w||^2 (team-wide).
+__device__ __noinline__ double team_axpy(const Team &tm, Cplx<float> *const *u, const double *coef, int nv,
+                            Cplx<float> *w, uint32_t n, BatchShared &S) {
+    double nrm = n >= STREAM_MIN ? axpy_pass<true>(tm, u, coef, nv, w, n)
+                                 : axpy_pass<false>(tm, u, coef, nv, w, n);
     proxy_fence_global();
     double dummy = 0.0;
     team_reduce(tm, nrm, dummy, true, S);
@@ -718,7 +758,7 @@ __global__ void __launch_bounds__(BT, 2) k_batch_otoc(const BatchArgs a) {
     R.git = 0;
     R.rgit = 0;
     R.sterms_w = reinterpret_cast<RowTerm<float> *>(base + a.stage_bytes);
-    R.sgroups_w = reinterpret_cast<RowGroup *>(base + a.stage_bytes + (a.table_bytes ? RMAXT * sizeof(RowTerm<float>) : 0));
+    R.sgroups_w = reinterpret_cast<RowGroup *>(base + a.stage_bytes + a.rterm_bytes);
     R.sterms = R.sterms_w;
     R.sgroups = R.sgroups_w;
     double *esmem = reinterpret_cast<double *>(base + a.stage_bytes + a.table_bytes);
@@ -805,8 +845,16 @@ static size_t stage_bytes(const BatchClass &c) {
     if (c.any_rows) b = std::max(b, (size_t)RS * RTILE);
     return (b + 1023) & ~(size_t)1023;
 }
+// Row tables sized for the class's largest term and group lists, not for
+// RMAXT: two CTAs per SM must leave room for the L1 share of the SM's
+// unified L1 / shared memory.  A 1.4 KB larger footprint that pushed two
+// CTAs from 194 to 197 KB (past the 196 KB carveout step) cost the row-tile
+// H.psi loop 12-19 %.
+static size_t rterm_bytes(const BatchClass &c) {
+    return c.any_rows ? (size_t)c.maxrt * sizeof(RowTerm<float>) : 0;
+}
 static size_t table_bytes(const BatchClass &c) {
-    return c.any_rows ? (size_t)RMAXT * (sizeof(RowTerm<float>) + sizeof(RowGroup)) : 0;
+    return c.any_rows ? rterm_bytes(c) + (((size_t)c.maxrg * sizeof(RowGroup) + 15) & ~(size_t)15) : 0;
 }
 static size_t dyn_smem(const BatchClass &c, int hcap) {
     return 1024 + stage_bytes(c) + table_bytes(c) + (size_t)(2 * hcap + 64) * sizeof(double);
@@ -932,6 +980,8 @@ void batch_build(BatchPlan &bp, int nprob, const int *len, const int64_t *nterms
         c.count++;
         if (probs[p].rows) {
             c.any_rows = true;
+            c.maxrt = std::max(c.maxrt, probs[p].rnterms);
+            c.maxrg = std::max(c.maxrg, probs[p].rngroups);
         } else {
             c.any_tiled = true;
             c.maxB = std::max(c.maxB, probs[p].B);
@@ -1014,6 +1064,7 @@ static BatchArgs class_args(const BatchPlan &bp, const BatchClass &c, int ntimes
     a.nvec = bp.krydim + 4;
     a.stage_bytes = stage_bytes(c);
     a.table_bytes = table_bytes(c);
+    a.rterm_bytes = rterm_bytes(c);
     return a;
 }
 

@@ -25,6 +25,7 @@ struct alignas(16) BatchProblem {
 // (clusters of `team` CTAs) of which `nslots` are resident.
 struct BatchClass {
     int team = 1, first = 0, count = 0, nslots = 0, maxB = 8, maxlen = 0;
+    int maxrt = 0, maxrg = 0;                // largest row-kernel term / group lists
     bool any_rows = false, any_tiled = false;
     size_t smem = 0, ws_stride = 0, vec_stride = 0;
     int map_base = 0;                        // first TMA map of this class's slots

@@ -336,3 +336,34 @@ def test_new_entry_points_reject_bad_arguments():
     b = SP.arnoldi(ham, x, 6)
     assert b.m_eff == 6
     ham.close()
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_apply_randomised_sweep(cuda, case):
+    """Seeded random draws over the whole kernel choice: state length 1-21
+    qubits (direct, bulk-copy tiled and TMA row kernels), 1-200 terms with
+    real, imaginary or mixed coefficients, Y-heavy strings (X and Z on the
+    same sites), both precisions, overwrite and accumulate."""
+    rng = np.random.default_rng(9000 + case)
+    L = int(rng.choice([1, 3, 7, 11, 13, 16, 17, 18, 19, 20, 21]))
+    dtype = ["c128", "c64"][case % 2]
+    kinds = ["mixed", "real", "imag"][case % 3]
+    T = int(rng.integers(1, 201))
+    bits, coeff = rand_terms(rng, L, T, kinds)
+    if case % 4 == 3:   # copy each X mask onto the Z bits: sigma^y on every flipped site
+        xm = np.zeros_like(bits)
+        for i in range(L):
+            xm |= bits & np.uint64(1 << (2 * i))
+        bits, idx = np.unique(xm | (xm << np.uint64(1)), return_index=True)
+        coeff = coeff[idx]
+    v = rand_vec(rng, L)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    x = to_dev(v, dtype)
+    out = torch.empty_like(x)
+    ham.apply(out, x)
+    ref = O.apply(L, bits, coeff, v)
+    tol = FP64_TOL if dtype == "c128" else FP32_TOL
+    got = out.cpu().numpy().astype(np.complex128)
+    assert relerr(got, ref) < tol, (L, dtype, kinds, len(bits), ham.info()["kernel"])
+    ham.apply(out, x, accumulate=True)
+    assert relerr(out.cpu().numpy().astype(np.complex128), 2 * ref) < tol
