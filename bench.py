@@ -513,7 +513,7 @@ def run_ours(args):
     hx.copy_(x.cpu())
     del y
     torch.cuda.empty_cache()
-    k2 = max(3, args.steps // 2)
+    k2 = max(3, args.steps)
     ham.apply_host(hy[:1], [hx])   # warm-up (allocates the pipeline buffers)
     barrier()
     torch.cuda.synchronize()

@@ -145,7 +145,12 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
  * elements of the Hamiltonian's precision each; pinned memory lets the
  * copies run asynchronously).  Pipelined over two device buffer pairs kept by
  * the library: the copy of state i+1 to the device and of result i-1 to the
- * host overlap H.psi on state i.  Returns when every result is on the host.
+ * host overlap H.psi on state i.  With the row kernel on large states
+ * (two or more CTA windows of output tiles: 2^22 complex64 or 2^21
+ * complex128 elements on a 148-SM B200) each product runs as up to 8
+ * launches over consecutive output ranges, and each range is copied back as
+ * soon as it is written.  Returns
+ * when every result is on the host.
  * No reference counterpart: the reference applies one resident state. */
 int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *out_host);
 

@@ -510,6 +510,7 @@ void apply_launch(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream_t st) 
     RP_REQUIRE(l.in != l.out, -2, "apply needs distinct input and output buffers");
     RP_REQUIRE(((uintptr_t)l.in & 15) == 0 && ((uintptr_t)l.out & 15) == 0, -2,
                "vectors must be 16-byte aligned");
+    RP_REQUIRE(l.tile_count == 0 || plan.rows.ok, -2, "output tile ranges need the row kernel");
     if (plan.cfg.direct) {
         RP_REQUIRE(l.ndot == 0, -2, "fused projections need the tiled kernel");
         const uint32_t D = 1u << plan.len;
@@ -552,6 +553,8 @@ void apply_launch(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream_t st) 
         r.ndot = l.ndot;
         r.partials = l.partials;
         r.err = l.err;
+        r.tile0 = l.tile0;
+        r.tile_count = l.tile_count;
         rows_launch(plan.rows, plan.len, plan.dtype, r, st);
         return;
     }

@@ -83,6 +83,9 @@ struct ApplyLaunch {
     int ndot = 0;
     double *partials = nullptr;   // [grid][ndot][2] compensated-summed per CTA
     unsigned *err = nullptr;      // device error word
+    // row kernel only: output tiles [tile0, tile0 + tile_count) of
+    // 2^plan.rows.B elements (tile_count 0: the whole state)
+    uint32_t tile0 = 0, tile_count = 0;
 };
 
 // Grid size used for a plan (persistent CTAs); the partials buffer of a fused

@@ -143,6 +143,7 @@ struct RowArgs {
     const RowTerm<float> *terms;
     const RowGroup *groups;
     int nterms, ngroups, ntiles, stages;
+    uint32_t tile0;          // first output tile of this launch (ntiles from there)
     double alpha;
     const double *alpha_dev;
     int accumulate;
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
                 }
                 const long ti = it / a.ngroups;
                 const int g = (int)(it - ti * a.ngroups);
-                const uint32_t o = blockIdx.x + (uint32_t)ti * gridDim.x;
+                const uint32_t o = a.tile0 + blockIdx.x + (uint32_t)ti * gridDim.x;
                 const uint32_t src = o ^ sgroups[g].xh;
                 mbar_arrive_expect_tx(&full[s], ROW_TILE_BYTES);
                 tma_load_2d(stage + (size_t)s * ROW_TILE_BYTES, &tmap, 0, (int)(src * 256u), &full[s]);
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
         long it = 0;
         bool ok = true;
         for (int ti = 0; ti < ntile_iters && ok; ++ti) {
-            const uint32_t o = blockIdx.x + (uint32_t)ti * gridDim.x;
+            const uint32_t o = a.tile0 + blockIdx.x + (uint32_t)ti * gridDim.x;
             Cplx<Real> acc[C];
 #pragma unroll
             for (int u = 0; u < C; u++) acc[u].x = acc[u].y = Real(0);
@@ -415,7 +416,8 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     a.groups = rp.d_groups;
     a.nterms = rp.nterms;
     a.ngroups = (int)rp.groups.size();
-    a.ntiles = rp.ntiles;
+    a.ntiles = l.tile_count ? (int)l.tile_count : rp.ntiles;
+    a.tile0 = l.tile0;
     a.stages = S;
     a.alpha = l.alpha;
     a.alpha_dev = l.alpha_dev;
@@ -433,6 +435,9 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st) {
     RP_REQUIRE(rp.ok, -2, "row kernel not planned for this Hamiltonian");
     RP_REQUIRE(l.ndot <= 64, -2, "too many fused projections");
+    RP_REQUIRE((uint64_t)l.tile0 + l.tile_count <= (uint64_t)rp.ntiles, -2, "output tile range out of bounds");
+    RP_REQUIRE(l.tile_count == 0 || l.ndot == 0, -2, "fused projections need the whole output");
+    RP_REQUIRE(l.tile_count != 0 || l.tile0 == 0, -2, "a tile offset needs a tile count");
     if (dtype == 2) launch_rows_t<double>(rp, len, dtype, l, st);
     else launch_rows_t<float>(rp, len, dtype, l, st);
 }

@@ -67,6 +67,9 @@ struct RowLaunch {
     int ndot = 0;
     double *partials = nullptr;   // [grid][ndot][2]
     unsigned *err = nullptr;
+    // output tiles [tile0, tile0 + tile_count) only (tile_count 0: all);
+    // every source tile stays readable
+    uint32_t tile0 = 0, tile_count = 0;
 };
 
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st);

@@ -347,12 +347,18 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate) {
     });
 }
 
+// Output chunks of rp_apply_host with the row kernel: each chunk's
+// device-to-host copy starts as soon as its output tiles are written, so
+// only the last chunk's copy follows the final product.
+constexpr int HOST_CHUNKS = 8;
+
 // Device buffers and streams of rp_apply_host, kept between calls.
 struct HostPipe {
     size_t bytes = 0;
     void *din[2] = {nullptr, nullptr}, *dout[2] = {nullptr, nullptr};
     cudaStream_t s_in = nullptr, s_out = nullptr;
     cudaEvent_t in_ready[2] = {}, comp_done[2] = {}, out_done[2] = {};
+    cudaEvent_t part_done[HOST_CHUNKS] = {};
 };
 static HostPipe g_pipe;
 
@@ -365,6 +371,8 @@ static void pipe_release() {
         if (p.comp_done[b]) cudaEventDestroy(p.comp_done[b]);
         if (p.out_done[b]) cudaEventDestroy(p.out_done[b]);
     }
+    for (int c = 0; c < HOST_CHUNKS; c++)
+        if (p.part_done[c]) cudaEventDestroy(p.part_done[c]);
     if (p.s_in) cudaStreamDestroy(p.s_in);
     if (p.s_out) cudaStreamDestroy(p.s_out);
     p = HostPipe{};
@@ -380,6 +388,8 @@ static void pipe_ensure(size_t bytes) {
             RP_CUDA(cudaEventCreateWithFlags(&p.comp_done[b], cudaEventDisableTiming));
             RP_CUDA(cudaEventCreateWithFlags(&p.out_done[b], cudaEventDisableTiming));
         }
+        for (int c = 0; c < HOST_CHUNKS; c++)
+            RP_CUDA(cudaEventCreateWithFlags(&p.part_done[c], cudaEventDisableTiming));
     }
     if (p.bytes >= bytes) return;
     for (int b = 0; b < 2; b++) {
@@ -404,6 +414,17 @@ int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *ou
         const size_t bytes = (size_t)esize(h->plan.dtype) << h->plan.len;
         pipe_ensure(bytes);
         HostPipe &p = g_pipe;
+        // output chunks: whole multiples of the row kernel's CTA window (the
+        // last chunk takes the rest); one chunk for the other kernels
+        const RowPlan &rp = h->plan.rows;
+        uint32_t per = 0;
+        int nch = 1;
+        if (rp.ok && rp.ntiles >= 2 * rp.window) {
+            const uint32_t waves = (uint32_t)((rp.ntiles + rp.window - 1) / rp.window);
+            per = (uint32_t)rp.window * ((waves + HOST_CHUNKS - 1) / HOST_CHUNKS);
+            nch = (int)((rp.ntiles + per - 1) / per);
+        }
+        const size_t tile_bytes = rp.ok ? (size_t)esize(h->plan.dtype) << rp.B : bytes;
         for (int i = 0; i < n; i++) {
             RP_REQUIRE(in_host[i] && out_host[i], RP_E_INVALID, "null host vector");
             const int b = i & 1;
@@ -414,13 +435,25 @@ int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *ou
             RP_CUDA(cudaStreamWaitEvent(g_stream, p.in_ready[b], 0));
             // the result buffer b is free once result i-2 reached the host
             if (i >= 2) RP_CUDA(cudaStreamWaitEvent(g_stream, p.out_done[b], 0));
-            ApplyLaunch L;
-            L.in = p.din[b];
-            L.out = p.dout[b];
-            apply_launch(h->plan, L, g_stream);
+            for (int c = 0; c < nch; c++) {
+                ApplyLaunch L;
+                L.in = p.din[b];
+                L.out = p.dout[b];
+                size_t off = 0, len = bytes;
+                if (nch > 1) {
+                    L.tile0 = (uint32_t)c * per;
+                    L.tile_count = std::min<uint32_t>(per, (uint32_t)rp.ntiles - L.tile0);
+                    off = (size_t)L.tile0 * tile_bytes;
+                    len = (size_t)L.tile_count * tile_bytes;
+                }
+                apply_launch(h->plan, L, g_stream);
+                RP_CUDA(cudaEventRecord(p.part_done[c], g_stream));
+                RP_CUDA(cudaStreamWaitEvent(p.s_out, p.part_done[c], 0));
+                RP_CUDA(cudaMemcpyAsync(static_cast<char *>(out_host[i]) + off,
+                                        static_cast<const char *>(p.dout[b]) + off, len,
+                                        cudaMemcpyDeviceToHost, p.s_out));
+            }
             RP_CUDA(cudaEventRecord(p.comp_done[b], g_stream));
-            RP_CUDA(cudaStreamWaitEvent(p.s_out, p.comp_done[b], 0));
-            RP_CUDA(cudaMemcpyAsync(out_host[i], p.dout[b], bytes, cudaMemcpyDeviceToHost, p.s_out));
             RP_CUDA(cudaEventRecord(p.out_done[b], p.s_out));
         }
         RP_CUDA(cudaStreamSynchronize(p.s_out));

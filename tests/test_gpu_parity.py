@@ -252,11 +252,13 @@ def test_ground_state_lanczos_matches_dense(model):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["c128", "c64"])
-def test_apply_host_pipeline_matches_device_apply(dtype):
+@pytest.mark.parametrize("L", [19, 22])
+def test_apply_host_pipeline_matches_device_apply(dtype, L):
     """rp_apply_host (host states, copies overlapped with the products) gives
-    the device apply's results for every state of the sequence."""
+    the device apply's results, bit for bit, for every state of the
+    sequence; at 22 qubits each product runs as several launches over output
+    ranges whose copies start as each range is written."""
     import reapers_b200 as rb
-    L = 19
     bits, coeff = rb.syk.sparse_syk(2 * L, 8, seed=2)
     ham = rb.Hamiltonian(L, bits, coeff, dtype)
     tdt = torch.complex128 if dtype == "c128" else torch.complex64
