@@ -252,6 +252,58 @@ def evolve_leg(seed=0, t=10.0, krydim=30, cpu=True):
     return out
 
 
+def shard_leg(ham, x, L, reps=3):
+    """The state split by its top k qubits into 2^k shards, k = 1..3, as
+    virtual shards on this GPU: every output shard by one peer-read launch
+    (rp_apply_shard, the kernel a rank runs on its own GPU with the other
+    shards in its peers' memory), all 2^k launches timed against the full
+    apply; results bit-identical to it.  peer_tile_fraction: the share of
+    source-tile loads a shard takes from other shards (terms whose X mask
+    reaches the top k qubits) -- the NVLink share of the loads on 2^k GPUs."""
+    import torch
+    import reapers_b200 as rb
+    st = rb.stream()
+    full = torch.empty_like(x)
+
+    def timed(fn):
+        fn()
+        rb.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_full = timed(lambda: ham.apply(full, x))
+    xm = rb.syk.xmask(np.asarray(ham.bits, dtype=np.uint64))
+    out = {"workload": f"the N=56 H.psi (2^{L} complex64) over 2^k virtual shards on one GPU, "
+                       f"one peer-read launch per output shard",
+           "full_apply_ms": round(t_full, 3), "shards": {}}
+    for k in (1, 2, 3):
+        n = x.numel() >> k
+        shards = [x[s * n:(s + 1) * n] for s in range(1 << k)]
+        outs = [torch.empty(n, dtype=x.dtype, device=x.device) for _ in shards]
+
+        def run():
+            for r in range(1 << k):
+                ham.apply_shard(outs[r], shards, rank=r)
+        t = timed(run)
+        same = all(torch.equal(outs[r], full[r * n:(r + 1) * n]) for r in range(1 << k))
+        rec = {"ms_all_shards": round(t, 3), "ms_per_shard": round(t / (1 << k), 3),
+               "vs_full_apply": round(t_full / t, 4), "bit_identical": bool(same)}
+        # source-tile groups (distinct x >> 12) whose shard offset x >> (L - k) is not 0
+        xh = np.unique(xm >> np.uint64(12))
+        rec["peer_tile_fraction"] = round(float(np.mean((xh >> np.uint64(L - k - 12)) != 0)), 4)
+        rec["terms_reaching_top_qubits"] = int(np.count_nonzero(xm >> np.uint64(L - k)))
+        out["shards"][f"k{k}"] = rec
+        del outs
+    del full
+    return out
+
+
 def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
               seq_per_size=2, tune=True):
     """Batched OTOC sample: nreal disorder realisations x nstates random
@@ -577,6 +629,8 @@ def run_ours(args):
         line["otoc_batched_syk32_40"] = batch_leg(seed=rank)
     if legs and args.config == "syk56" and not args.no_steps:
         line["learned_steps"] = step_leg(seed=rank)
+    if legs and args.config == "syk56" and not args.no_shard:
+        line["sharded_peer_syk56"] = shard_leg(ham, x, L)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
@@ -652,6 +706,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="syk56")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-shard", action="store_true",
+                    help="skip the peer-read sharded H.psi leg (virtual shards on one GPU)")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched OTOC leg (sparse SYK N = 32/36/40)")
     ap.add_argument("--no-evolve", action="store_true", help="skip the N = 48 FP64 vs mixed evolve leg")

@@ -154,6 +154,33 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
  * No reference counterpart: the reference applies one resident state. */
 int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *out_host);
 
+/* The reference's multi-GPU apply (src/krnl.cu:96-114 with the split of
+ * inc/gpuimpl.h:426-432): the state is split by its top shard_bits qubits
+ * into 2^shard_bits shards of 2^(len-shard_bits) elements; shards[i] is a
+ * device pointer to input shard i readable from this device (this GPU's
+ * memory, or a peer's opened with rp_ipc_open), and out (2^(len-shard_bits)
+ * elements) becomes output shard shard_rank of H in, or += with accumulate.
+ * One launch of the row kernel: its TMA loads fetch every source tile from
+ * the shard that holds it, over NVLink for a peer's.  1 <= shard_bits <= 3;
+ * needs the row kernel (2^19+ complex64 or 2^18+ complex128 elements) with
+ * at least one 2^12 (complex64) or 2^11 (complex128) element tile per shard.
+ * The caller orders it: every shard final before the call (a barrier across
+ * ranks), and no input shard rewritten until every rank's call has ended. */
+int rp_apply_shard(rp_ham_t h, int shard_bits, int shard_rank, const void *const *shards,
+                   void *out, int accumulate);
+
+/* One process per GPU in place of the reference's in-process peer access
+ * (inc/gpuimpl.h:524-538): a device pointer exported as the CUDA IPC handle
+ * of its allocation plus its offset, opened in another process (peer access
+ * enabled lazily) and closed there. */
+typedef struct {
+    unsigned char handle[64];
+    uint64_t offset;
+} rp_ipc_handle_t;
+int rp_ipc_export(const void *ptr, rp_ipc_handle_t *out);
+int rp_ipc_open(const rp_ipc_handle_t *h, void **ptr);
+int rp_ipc_close(void *ptr);
+
 /* Krylov<Impl>::evolve (inc/algo.h:267-365) as called by State::evolve
  * (inc/state.h:415-424): psi <- exp(-(beta + i t) H) psi in place, restarted
  * Arnoldi with krydim basis vectors, stop when ||Hexp0|| < tol, on breakdown,

@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import RP_C64, RP_C128, RPError
 from . import syk  # noqa: F401  (term generators)
 
-__all__ = ["Hamiltonian", "evolve", "ground_state", "dot", "norm", "axpy", "scale", "random_state",
+__all__ = ["Hamiltonian", "evolve", "ground_state", "ipc_export", "ipc_open", "ipc_close", "dot", "norm", "axpy", "scale", "random_state",
            "stream", "synchronize", "RPError", "RP_C64", "RP_C128", "dtype_code", "syk",
            "otoc", "otoc_block"]
 
@@ -122,6 +122,35 @@ class Hamiltonian:
         _lib.call("rp_apply_host", self._h, n, ip, op)
         return outs
 
+    def apply_shard(self, out, shards, accumulate=False, rank=None):
+        """out = output shard `rank` of H applied to the state whose 2^k
+        shards (top k qubits, k = log2 len(shards)) are the device tensors or
+        raw device pointers `shards`; a shard may be a peer's memory (see
+        ``ipc_export`` / ``ipc_open``).  One row-kernel launch reading every
+        source tile from the shard that holds it (rp_apply_shard)."""
+        n = len(shards)
+        k = n.bit_length() - 1
+        if n < 2 or 1 << k != n:
+            raise ValueError("the number of shards must be a power of two, at least 2")
+        if rank is None or not 0 <= rank < n:
+            raise ValueError("rank must name one of the shards")
+        want = 1 << (self.len - k)
+        if _tcode(out) != self.dtype or out.numel() != want:
+            raise ValueError("the output shard must have 2^(len - k) elements of the "
+                             "Hamiltonian's precision")
+        ptrs = []
+        for t in shards:
+            if isinstance(t, int):
+                ptrs.append(t)
+            else:
+                if _tcode(t) != self.dtype or t.numel() != want or not t.is_contiguous():
+                    raise ValueError("every shard must be a contiguous 2^(len - k) vector of "
+                                     "the Hamiltonian's precision")
+                ptrs.append(_ptr(t).value)
+        arr = (C.c_void_p * n)(*ptrs)
+        _lib.call("rp_apply_shard", self._h, k, rank, arr, _ptr(out), 1 if accumulate else 0)
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().rp_ham_destroy(self._h)
@@ -195,6 +224,30 @@ def ground_state(ham, krydim=5, eps=None, maxiter=0, seed=0):
         v0 = g
         if not (beta and beta[0] > eps and (not maxiter or numiter < maxiter)):
             return float(evals[idx]), g
+
+
+def ipc_export(t):
+    """A device tensor (or raw device pointer) as (64-byte CUDA IPC handle of
+    its allocation, offset) for another process on this node."""
+    h = _lib.IpcHandle()
+    _lib.call("rp_ipc_export", t if isinstance(t, int) else _ptr(t), C.byref(h))
+    return bytes(h.handle), int(h.offset)
+
+
+def ipc_open(handle):
+    """The device pointer of another process's exported tensor (an
+    ``ipc_export`` result), peer access enabled; release with ``ipc_close``."""
+    data, offset = handle
+    h = _lib.IpcHandle()
+    C.memmove(h.handle, data, 64)
+    h.offset = offset
+    p = C.c_void_p()
+    _lib.call("rp_ipc_open", C.byref(h), C.byref(p))
+    return p.value
+
+
+def ipc_close(ptr):
+    _lib.call("rp_ipc_close", ptr)
 
 
 def dot(a, b):

@@ -39,6 +39,10 @@ class EvolveStats(C.Structure):
                 ("prods", C.c_int), ("breakdown", C.c_int), ("last_err", C.c_double)]
 
 
+class IpcHandle(C.Structure):
+    _fields_ = [("handle", C.c_ubyte * 64), ("offset", C.c_uint64)]
+
+
 class ArnoldiInfo(C.Structure):
     _fields_ = [("m_eff", C.c_int), ("breakdown", C.c_int), ("passes", C.c_int),
                 ("pad", C.c_int), ("beta", C.c_double),
@@ -74,6 +78,10 @@ _SIGS = {
     "rp_ham_info": (C.c_int, [_VP, C.POINTER(HamInfo)]),
     "rp_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "rp_apply_host": (C.c_int, [_VP, C.c_int, C.POINTER(_VP), C.POINTER(_VP)]),
+    "rp_apply_shard": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(_VP), _VP, C.c_int]),
+    "rp_ipc_export": (C.c_int, [_VP, C.POINTER(IpcHandle)]),
+    "rp_ipc_open": (C.c_int, [C.POINTER(IpcHandle), C.POINTER(_VP)]),
+    "rp_ipc_close": (C.c_int, [_VP]),
     "rp_evolve": (C.c_int, [_VP, _VP, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                             C.POINTER(EvolveStats)]),
     "rp_workspace_release": (C.c_int, []),

@@ -506,6 +506,27 @@ static void dispatch_B(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream_t
 }
 
 void apply_launch(const ApplyPlan &plan, const ApplyLaunch &l, cudaStream_t st) {
+    if (l.shards) {
+        RP_REQUIRE(plan.rows.ok, -2,
+                   "a sharded apply needs the row kernel: states of at least 2^19 complex64 or "
+                   "2^18 complex128 elements, at most 2048 terms after splitting complex "
+                   "coefficients");
+        RP_REQUIRE(l.out && ((uintptr_t)l.out & 15) == 0, -2, "the output shard must be 16-byte aligned");
+        RowLaunch r;
+        r.out = l.out;
+        r.alpha = l.alpha;
+        r.alpha_dev = l.alpha_dev;
+        r.accumulate = l.accumulate;
+        r.active = l.active;
+        r.err = l.err;
+        r.tile0 = l.tile0;
+        r.tile_count = l.tile_count;
+        r.shards = l.shards;
+        r.shard_bits = l.shard_bits;
+        r.shard_rank = l.shard_rank;
+        rows_launch(plan.rows, plan.len, plan.dtype, r, st);
+        return;
+    }
     RP_REQUIRE(l.in && l.out, -2, "null vector pointer");
     RP_REQUIRE(l.in != l.out, -2, "apply needs distinct input and output buffers");
     RP_REQUIRE(((uintptr_t)l.in & 15) == 0 && ((uintptr_t)l.out & 15) == 0, -2,

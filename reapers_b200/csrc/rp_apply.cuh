@@ -86,6 +86,10 @@ struct ApplyLaunch {
     // row kernel only: output tiles [tile0, tile0 + tile_count) of
     // 2^plan.rows.B elements (tile_count 0: the whole state)
     uint32_t tile0 = 0, tile_count = 0;
+    // row kernel only: the input split into 2^shard_bits shards (in unused),
+    // out = output shard shard_rank; see RowLaunch
+    const void *const *shards = nullptr;
+    int shard_bits = 0, shard_rank = 0;
 };
 
 // Grid size used for a plan (persistent CTAs); the partials buffer of a fused

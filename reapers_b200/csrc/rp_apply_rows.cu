@@ -144,6 +144,10 @@ struct RowArgs {
     const RowGroup *groups;
     int nterms, ngroups, ntiles, stages;
     uint32_t tile0;          // first output tile of this launch (ntiles from there)
+    // sharded launch: output tiles are local tiles of shard gtile0 >> lbits;
+    // source tile s (global) is local tile s & (2^lbits - 1) of map s >> lbits
+    uint32_t gtile0;
+    int lbits, nmaps;
     double alpha;
     const double *alpha_dev;
     int accumulate;
@@ -158,9 +162,11 @@ constexpr int ROW_P = 256;          // consumer threads = rows per tile
 constexpr int ROW_NW = ROW_P / 32;
 constexpr unsigned ROW_TILE_BYTES = 256 * 128;
 
-template <typename Real, int MINB>
-__global__ void __launch_bounds__(ROW_P + 32, MINB)
-    k_apply_rows(const __grid_constant__ CUtensorMap tmap, const RowArgs<Real> a) {
+// The row kernel's body.  maps points at kernel-parameter tensor maps: one
+// over the whole input state, or (SHARD) one per input shard, a shard being
+// this GPU's memory or a peer's.
+template <typename Real, bool SHARD>
+__device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const RowArgs<Real> a) {
     constexpr int C = 128 / (int)sizeof(Cplx<Real>);   // elements per row
     constexpr int LOGC = C == 16 ? 4 : 3;
     constexpr int B = LOGC + 8;
@@ -201,8 +207,9 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
 
     if (warp == ROW_NW) {
         if (lane == 0) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap))
-                         : "memory");
+            for (int i = 0; i < (SHARD ? a.nmaps : 1); i++)
+                asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps[i]))
+                             : "memory");
             long it = 0;
             for (; it < total; ++it) {
                 const int s = (int)(it % S);
@@ -214,9 +221,16 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
                 const long ti = it / a.ngroups;
                 const int g = (int)(it - ti * a.ngroups);
                 const uint32_t o = a.tile0 + blockIdx.x + (uint32_t)ti * gridDim.x;
-                const uint32_t src = o ^ sgroups[g].xh;
                 mbar_arrive_expect_tx(&full[s], ROW_TILE_BYTES);
-                tma_load_2d(stage + (size_t)s * ROW_TILE_BYTES, &tmap, 0, (int)(src * 256u), &full[s]);
+                if constexpr (SHARD) {
+                    const uint32_t src = (a.gtile0 + o) ^ sgroups[g].xh;
+                    const uint32_t lsrc = src & ((1u << a.lbits) - 1u);
+                    tma_load_2d(stage + (size_t)s * ROW_TILE_BYTES, &maps[src >> a.lbits], 0,
+                                (int)(lsrc * 256u), &full[s]);
+                } else {
+                    const uint32_t src = o ^ sgroups[g].xh;
+                    tma_load_2d(stage + (size_t)s * ROW_TILE_BYTES, maps, 0, (int)(src * 256u), &full[s]);
+                }
             }
             s_issued = it;
         }
@@ -227,6 +241,7 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
         bool ok = true;
         for (int ti = 0; ti < ntile_iters && ok; ++ti) {
             const uint32_t o = a.tile0 + blockIdx.x + (uint32_t)ti * gridDim.x;
+            const uint32_t og = SHARD ? a.gtile0 + o : o;   // global tile: the Z signs
             Cplx<Real> acc[C];
 #pragma unroll
             for (int u = 0; u < C; u++) acc[u].x = acc[u].y = Real(0);
@@ -234,7 +249,7 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
                 const int s = (int)(it % S);
                 const unsigned round = (unsigned)(it / S);
                 const RowGroup gd = sgroups[g];
-                const uint32_t src_hi = (o ^ gd.xh) << B;
+                const uint32_t src_hi = (og ^ gd.xh) << B;
                 if (!mbar_wait_bounded(&full[s], round & 1u, a.err)) {
                     ok = false;
                     break;
@@ -352,9 +367,34 @@ __global__ void __launch_bounds__(ROW_P + 32, MINB)
     }
 }
 
+template <typename Real, int MINB>
+__global__ void __launch_bounds__(ROW_P + 32, MINB)
+    k_apply_rows(const __grid_constant__ CUtensorMap tmap, const RowArgs<Real> a) {
+    apply_rows_body<Real, false>(&tmap, a);
+}
+
+// One output shard of a state split by its top qubits: the source tiles come
+// from the shard that holds them (plain TMA loads, over NVLink for a peer's
+// memory; no multicast).
+struct RowShardMaps {
+    CUtensorMap m[ROW_MAX_SHARDS];
+};
+
+template <typename Real, int MINB>
+__global__ void __launch_bounds__(ROW_P + 32, MINB)
+    k_apply_rows_shard(const __grid_constant__ RowShardMaps maps, const RowArgs<Real> a) {
+    apply_rows_body<Real, true>(maps.m, a);
+}
+
 // ---------------------------------------------------------------------------
 // Host launch
 // ---------------------------------------------------------------------------
+static int ilog2(uint32_t v) {
+    int r = 0;
+    while ((2u << r) <= v) r++;
+    return r;
+}
+
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
@@ -404,20 +444,30 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     int S = (int)std::min<size_t>(6, (budget - fixed - 16 * 8) / (ROW_TILE_BYTES + 16));
     RP_REQUIRE(S >= 2, -2, "Hamiltonian table too large for the row kernel");
     const size_t smem = (size_t)S * ROW_TILE_BYTES + fixed + (size_t)2 * S * sizeof(uint64_t);
+    const bool shard = l.shards != nullptr;
     auto kern = ctas == 2 ? k_apply_rows<Real, 2> : k_apply_rows<Real, 1>;
-    static size_t attr[2] = {0, 0};
-    if (smem > attr[ctas - 1]) {
-        RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr[ctas - 1] = smem;
+    auto kern_sh = ctas == 2 ? k_apply_rows_shard<Real, 2> : k_apply_rows_shard<Real, 1>;
+    static size_t attr[2][2] = {{0, 0}, {0, 0}};
+    if (smem > attr[shard][ctas - 1]) {
+        if (shard)
+            RP_CUDA(cudaFuncSetAttribute(kern_sh, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        else
+            RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr[shard][ctas - 1] = smem;
     }
+    const int lbits = shard ? ilog2((uint32_t)rp.ntiles) - l.shard_bits : 0;
+    const int local_tiles = shard ? rp.ntiles >> l.shard_bits : rp.ntiles;
     RowArgs<Real> a;
     a.out = static_cast<Cplx<Real> *>(l.out);
     a.terms = static_cast<const RowTerm<float> *>(rp.d_terms);
     a.groups = rp.d_groups;
     a.nterms = rp.nterms;
     a.ngroups = (int)rp.groups.size();
-    a.ntiles = l.tile_count ? (int)l.tile_count : rp.ntiles;
+    a.ntiles = l.tile_count ? (int)l.tile_count : local_tiles;
     a.tile0 = l.tile0;
+    a.gtile0 = shard ? (uint32_t)l.shard_rank << lbits : 0u;
+    a.lbits = lbits;
+    a.nmaps = shard ? 1 << l.shard_bits : 1;
     a.stages = S;
     a.alpha = l.alpha;
     a.alpha_dev = l.alpha_dev;
@@ -427,15 +477,36 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     a.ndot = l.ndot;
     a.partials = l.partials;
     a.err = l.err;
-    const CUtensorMap map = make_row_map(l.in, len, dtype);
-    kern<<<rp.window, ROW_P + 32, smem, st>>>(map, a);
+    if (shard) {
+        RowShardMaps maps;
+        std::memset(&maps, 0, sizeof(maps));
+        for (int i = 0; i < a.nmaps; i++) maps.m[i] = make_row_map(l.shards[i], len - l.shard_bits, dtype);
+        kern_sh<<<std::min(rp.window, local_tiles), ROW_P + 32, smem, st>>>(maps, a);
+    } else {
+        const CUtensorMap map = make_row_map(l.in, len, dtype);
+        kern<<<rp.window, ROW_P + 32, smem, st>>>(map, a);
+    }
     RP_CUDA(cudaGetLastError());
 }
 
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st) {
     RP_REQUIRE(rp.ok, -2, "row kernel not planned for this Hamiltonian");
     RP_REQUIRE(l.ndot <= 64, -2, "too many fused projections");
-    RP_REQUIRE((uint64_t)l.tile0 + l.tile_count <= (uint64_t)rp.ntiles, -2, "output tile range out of bounds");
+    if (l.shards) {
+        RP_REQUIRE(l.shard_bits >= 1 && l.shard_bits <= ilog2(ROW_MAX_SHARDS), -2,
+                   "a sharded apply takes 2 to " + std::to_string(ROW_MAX_SHARDS) + " shards");
+        RP_REQUIRE(rp.ntiles >= (1 << l.shard_bits), -2,
+                   "every shard must hold at least one row tile (2^" + std::to_string(rp.B) + " elements)");
+        RP_REQUIRE(l.shard_rank >= 0 && l.shard_rank < (1 << l.shard_bits), -2, "shard index out of range");
+        RP_REQUIRE(l.ndot == 0, -2, "fused projections are not taken in a sharded apply");
+        for (int i = 0; i < (1 << l.shard_bits); i++) {
+            RP_REQUIRE(l.shards[i] && ((uintptr_t)l.shards[i] & 15) == 0, -2,
+                       "shard pointers must be non-null and 16-byte aligned");
+            RP_REQUIRE(l.shards[i] != l.out, -2, "the output may not be an input shard");
+        }
+    }
+    const uint64_t out_tiles = l.shards ? (uint64_t)rp.ntiles >> l.shard_bits : (uint64_t)rp.ntiles;
+    RP_REQUIRE((uint64_t)l.tile0 + l.tile_count <= out_tiles, -2, "output tile range out of bounds");
     RP_REQUIRE(l.tile_count == 0 || l.ndot == 0, -2, "fused projections need the whole output");
     RP_REQUIRE(l.tile_count != 0 || l.tile0 == 0, -2, "a tile offset needs a tile count");
     if (dtype == 2) launch_rows_t<double>(rp, len, dtype, l, st);

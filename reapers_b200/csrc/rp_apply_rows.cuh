@@ -70,7 +70,14 @@ struct RowLaunch {
     // output tiles [tile0, tile0 + tile_count) only (tile_count 0: all);
     // every source tile stays readable
     uint32_t tile0 = 0, tile_count = 0;
+    // sharded input (in unused): shards[i], i < 2^shard_bits, holds input
+    // elements [i 2^(len-shard_bits), (i+1) 2^(len-shard_bits)); out is
+    // output shard shard_rank
+    const void *const *shards = nullptr;
+    int shard_bits = 0, shard_rank = 0;
 };
+
+constexpr int ROW_MAX_SHARDS = 8;
 
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st);
 

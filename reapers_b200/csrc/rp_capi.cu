@@ -1,8 +1,12 @@
 // C ABI of librpb200.so: argument checking, error translation, context.
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "../../include/rpb200.h"
 #include "rp_apply.cuh"
@@ -344,6 +348,93 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate) {
         L.out = out;
         L.accumulate = accumulate;
         apply_launch(h->plan, L, g_stream);
+    });
+}
+
+int rp_apply_shard(rp_ham_t h, int shard_bits, int shard_rank, const void *const *shards, void *out,
+                   int accumulate) {
+    return guarded([&] {
+        RP_REQUIRE(h && shards, RP_E_INVALID, "null argument");
+        check_vec(out);
+        ApplyLaunch L;
+        L.out = out;
+        L.accumulate = accumulate;
+        L.shards = shards;
+        L.shard_bits = shard_bits;
+        L.shard_rank = shard_rank;
+        apply_launch(h->plan, L, g_stream);
+    });
+}
+
+// CUDA IPC: a device pointer travels as the handle of its allocation plus
+// its offset inside it (torch's caching allocator hands out interior
+// pointers), and is opened with peer access enabled lazily.
+static_assert(sizeof(cudaIpcMemHandle_t) == sizeof(((rp_ipc_handle_t *)0)->handle), "IPC handle size");
+
+static PFN_cuMemGetAddressRange_v3020 get_address_range() {
+    static PFN_cuMemGetAddressRange_v3020 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        RP_CUDA(cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q));
+        RP_REQUIRE(q == cudaDriverEntryPointSuccess && p, RP_E_CUDA, "cuMemGetAddressRange unavailable");
+        fn = reinterpret_cast<PFN_cuMemGetAddressRange_v3020>(p);
+    }
+    return fn;
+}
+
+// Opened allocations by handle (an allocation may hold several exported
+// tensors: it is mapped once and reference-counted), and the allocation of
+// every pointer handed out.
+static std::map<std::string, std::pair<void *, int>> g_ipc_bases;
+static std::multimap<void *, std::string> g_ipc_ptrs;
+
+int rp_ipc_export(const void *ptr, rp_ipc_handle_t *out) {
+    return guarded([&] {
+        RP_REQUIRE(ptr && out, RP_E_INVALID, "null argument");
+        CUdeviceptr base = 0;
+        size_t size = 0;
+        const CUresult r = get_address_range()(&base, &size, (CUdeviceptr)(uintptr_t)ptr);
+        RP_REQUIRE(r == CUDA_SUCCESS, RP_E_INVALID, "not a device allocation (cuMemGetAddressRange " +
+                                                        std::to_string((int)r) + ")");
+        cudaIpcMemHandle_t hd;
+        RP_CUDA(cudaIpcGetMemHandle(&hd, reinterpret_cast<void *>(base)));
+        std::memcpy(out->handle, &hd, sizeof(hd));
+        out->offset = (uint64_t)((uintptr_t)ptr - (uintptr_t)base);
+    });
+}
+
+int rp_ipc_open(const rp_ipc_handle_t *h, void **ptr) {
+    return guarded([&] {
+        RP_REQUIRE(h && ptr, RP_E_INVALID, "null argument");
+        const std::string key(reinterpret_cast<const char *>(h->handle), sizeof(h->handle));
+        auto it = g_ipc_bases.find(key);
+        if (it == g_ipc_bases.end()) {
+            cudaIpcMemHandle_t hd;
+            std::memcpy(&hd, h->handle, sizeof(hd));
+            void *base = nullptr;
+            RP_CUDA(cudaIpcOpenMemHandle(&base, hd, cudaIpcMemLazyEnablePeerAccess));
+            it = g_ipc_bases.emplace(key, std::make_pair(base, 0)).first;
+        }
+        it->second.second++;
+        void *p = static_cast<char *>(it->second.first) + h->offset;
+        g_ipc_ptrs.emplace(p, key);
+        *ptr = p;
+    });
+}
+
+int rp_ipc_close(void *ptr) {
+    return guarded([&] {
+        auto it = g_ipc_ptrs.find(ptr);
+        RP_REQUIRE(it != g_ipc_ptrs.end(), RP_E_INVALID, "pointer was not opened by rp_ipc_open");
+        const std::string key = it->second;
+        g_ipc_ptrs.erase(it);
+        auto b = g_ipc_bases.find(key);
+        if (--b->second.second == 0) {
+            void *base = b->second.first;
+            g_ipc_bases.erase(b);
+            RP_CUDA(cudaIpcCloseMemHandle(base));
+        }
     });
 }
 

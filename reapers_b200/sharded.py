@@ -73,6 +73,9 @@ class LocalComm:
     def allreduce(self, arr):
         return np.asarray(arr, dtype=np.float64)
 
+    def barrier(self):
+        pass
+
 
 class ProcessGroupComm:
     """One shard per rank of a torch.distributed process group."""
@@ -89,9 +92,15 @@ class ProcessGroupComm:
 
     def start_exchange(self, send, peer, recv):
         """Swap `send` with rank `peer` into `recv`; returns the pending requests."""
+        return self.start_exchanges([(send, peer, recv)])
+
+    def start_exchanges(self, swaps):
+        """Every (send, peer, recv) swap at once; returns the pending requests."""
         d = self.dist
-        ops = [d.P2POp(d.isend, send, peer, self.group), d.P2POp(d.irecv, recv, peer, self.group)]
-        return d.batch_isend_irecv(ops)
+        ops = []
+        for send, peer, recv in swaps:
+            ops += [d.P2POp(d.isend, send, peer, self.group), d.P2POp(d.irecv, recv, peer, self.group)]
+        return d.batch_isend_irecv(ops) if ops else []
 
     def allreduce(self, arr):
         import torch
@@ -100,6 +109,22 @@ class ProcessGroupComm:
         t = torch.from_numpy(a.copy()).to(dev)
         self.dist.all_reduce(t, group=self.group)
         return t.cpu().numpy()
+
+    def all_gather_object(self, obj):
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj, group=self.group)
+        return out
+
+    def barrier(self):
+        """Every rank's device work issued so far is complete when this
+        returns (the library stream and torch's are synchronised first)."""
+        import torch
+        from . import synchronize
+        synchronize()
+        torch.cuda.synchronize()
+        self.dist.barrier(group=self.group)
+        if self.dist.get_backend(self.group) == "nccl":
+            torch.cuda.synchronize()
 
 
 class Shards:
@@ -125,22 +150,87 @@ class Shards:
         import torch
         return torch.cat([self.t[r] for r in sorted(self.t)])
 
+    peers = None      # device pointers of every shard, for peer-read applies
+    _opened = ()
+
+    def share(self):
+        """Make every shard readable by every rank (collective): with one
+        process per GPU the shards are exported as CUDA IPC handles and the
+        peers' opened; in one process the pointers are taken as they are."""
+        from . import ipc_export, ipc_open, _ptr
+        if isinstance(self.comm, LocalComm):
+            self.peers = [_ptr(self.t[r]).value for r in range(self.comm.world)]
+            return self
+        (r, t), = self.t.items()
+        handles = self.comm.all_gather_object(ipc_export(t))
+        ptrs, opened = [], []
+        for i, h in enumerate(handles):
+            if i == r:
+                ptrs.append(_ptr(t).value)
+            else:
+                p = ipc_open(h)
+                ptrs.append(p)
+                opened.append(p)
+        self.peers, self._opened = ptrs, tuple(opened)
+        return self
+
+    def unshare(self):
+        """Close the peers' mappings (collective; afterwards a rank may free
+        its shard)."""
+        from . import ipc_close
+        for p in self._opened:
+            ipc_close(p)
+        self.peers, self._opened = None, ()
+        self.comm.barrier()
+
 
 class ShardedHamiltonian:
     """H over 2^k shards of an L-qubit state: the local Hamiltonians
     H_xh^(r) of every owned shard r, on the single-GPU kernels."""
 
-    def __init__(self, L, bits, coeff, comm, dtype="c128", local=None):
+    def __init__(self, L, bits, coeff, comm, dtype="c128", local=None, exchange="copy", full=None):
         """local: the operator class of one shard's terms, called as
         local(length, bits, coeff, dtype) and providing apply(out, inp,
-        accumulate) and close(); the library's Hamiltonian unless given."""
+        accumulate) and close(); the library's Hamiltonian unless given.
+
+        exchange: "copy" swaps partner shards into local buffers (NCCL
+        send/recv, or plain reads in one process) one at a time, each swap
+        in flight while the previous local Hamiltonian is applied; "peer"
+        applies the full Hamiltonian in one row-kernel launch per output
+        shard that reads every source tile straight from the shard holding
+        it (rp_apply_shard: over NVLink for a peer's memory, inputs made
+        readable with Shards.share()); "stage" swaps every partner shard the
+        terms need at once (each crosses NVLink once) and then runs that same
+        single launch over the local copies.
+
+        full: for "peer" / "stage", the class of the full operator, called
+        as full(length, bits, coeff, dtype) and providing
+        apply_shard(out, shards, rank=r) and close(); the library's
+        Hamiltonian unless given."""
         from . import Hamiltonian
         local = local or Hamiltonian
         k = int(round(math.log2(comm.world)))
         if 1 << k != comm.world:
             raise ValueError("the number of shards must be a power of two")
+        if exchange not in ("copy", "peer", "stage"):
+            raise ValueError("exchange must be 'copy', 'peer' or 'stage'")
         self.L, self.k, self.comm, self.dtype = L, k, comm, dtype
+        self.exchange = exchange
         self.parts = {}
+        if exchange in ("peer", "stage"):
+            if k < 1:
+                raise ValueError("a single-launch sharded apply needs at least two shards")
+            self.full = (full or Hamiltonian)(L, bits, coeff, dtype)
+            if full is None and self.full.info()["kernel"] != 2:
+                self.full.close()
+                raise ValueError("a single-launch sharded apply needs the row kernel (2^19+ "
+                                 "complex64 or 2^18+ complex128 elements)")
+            # shard offsets the terms reach (the top k bits of their X masks)
+            xs = (S.xmask(np.asarray(bits, dtype=np.uint64)) >> np.uint64(L - k)).astype(np.int64)
+            self.offsets = sorted(set(xs.tolist()) - {0})
+            self.xhs = []
+            self._stage = {}
+            return
         for r in comm.owned():
             self.parts[r] = [(h, local(L - k, b, c, dtype))
                              for h, (b, c) in shard_terms(L, k, bits, coeff, r).items()]
@@ -150,6 +240,38 @@ class ShardedHamiltonian:
     def apply(self, out, inp):
         """out = H inp (Shards of the same layout)."""
         import torch
+        if self.exchange == "peer":
+            local = isinstance(self.comm, LocalComm)
+            ptrs = inp.peers
+            if ptrs is None:
+                if not local:
+                    raise ValueError("share() the input shards before a peer-read apply")
+                ptrs = [inp.t[s] for s in range(self.comm.world)]
+            # every shard final before any rank reads it, and read by every
+            # rank before any rank goes on to overwrite one
+            self.comm.barrier()
+            for r in out.t:
+                self.full.apply_shard(out.t[r], ptrs, rank=r)
+            self.comm.barrier()
+            return out
+        if self.exchange == "stage":
+            if isinstance(self.comm, LocalComm):
+                shards = [inp.t[s] for s in range(self.comm.world)]
+                for r in out.t:
+                    self.full.apply_shard(out.t[r], shards, rank=r)
+                return out
+            (r, src), = inp.t.items()
+            for d in self.offsets:
+                buf = self._stage.get(d)
+                if buf is None or buf.shape != src.shape or buf.dtype != src.dtype:
+                    self._stage[d] = torch.empty_like(src)
+            reqs = self.comm.start_exchanges([(src, r ^ d, self._stage[d]) for d in self.offsets])
+            for q in reqs:
+                q.wait()
+            # shards no term reaches are never read: any valid vector stands in
+            shards = [src if s == r else self._stage.get(r ^ s, src) for s in range(self.comm.world)]
+            self.full.apply_shard(out.t[r], shards, rank=r)
+            return out
         if isinstance(self.comm, LocalComm):
             for r, parts in self.parts.items():
                 first = True
@@ -196,6 +318,9 @@ class ShardedHamiltonian:
         for parts in self.parts.values():
             for _, h in parts:
                 h.close()
+        if self.exchange in ("peer", "stage"):
+            self.full.close()
+            self._stage = {}
 
 
 def sharded_dot(a, b):
@@ -243,6 +368,10 @@ def sharded_evolve(ham, psi, t, beta=0.0, krydim=5, tol=None, max_iters=0):
     if beta0 == 0.0:
         return {"restarts": 0, "applies": 0, "passes": 0}
     V = [Shards.empty_like(psi) for _ in range(m + 1)]
+    peer = getattr(ham, "exchange", "copy") == "peer"
+    if peer:
+        for v in V:
+            v.share()
     for r in psi.t:
         V[0].t[r].copy_(psi.t[r])
     _scale(V[0], 1.0 / beta0)
@@ -309,4 +438,7 @@ def sharded_evolve(ham, psi, t, beta=0.0, krydim=5, tol=None, max_iters=0):
         oldbeta = nrm_w
     for r in psi.t:
         psi.t[r].copy_(y.t[r])
+    if peer:
+        for v in V:
+            v.unshare()
     return stats

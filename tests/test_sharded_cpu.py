@@ -3,9 +3,10 @@
 * the per-shard local Hamiltonians H_xh^(r) reassemble the full operator:
   block (r, r ^ xh) of the oracle's dense matrix equals the dense matrix of
   H_xh^(r) on L - k qubits;
-* the exchange schedule of ShardedHamiltonian.apply over real gloo process
-  groups (world size 2 and 4): every rank swaps shards with r ^ xh in the
-  same order, and the gathered result equals the full dense product.  The
+* the exchange schedules of ShardedHamiltonian.apply over real gloo process
+  groups (world size 2 and 4): one swap with r ^ xh at a time ("copy"), or
+  every needed partner shard at once before one full-operator launch
+  ("stage"); the gathered result equals the full dense product.  The
   local products here are dense numpy matrices from the oracle (the checker)
   injected through ShardedHamiltonian's `local` argument; on the GPU they
   are the library's kernels (tests/test_gpu_sharded.py).
@@ -62,20 +63,42 @@ class _DenseLocal:
         pass
 
 
+class _DenseFull:
+    """Dense numpy stand-in for the full operator's single-launch sharded
+    apply (test only): output shard `rank` from the concatenated shards."""
+
+    def __init__(self, length, bits, coeff, dtype):
+        self.M = torch.from_numpy(O.dense_matrix(length, bits, coeff))
+
+    def apply_shard(self, out, shards, rank, accumulate=False):
+        n = out.numel()
+        r = self.M[rank * n:(rank + 1) * n] @ torch.cat(list(shards))
+        if accumulate:
+            out += r
+        else:
+            out.copy_(r)
+
+    def close(self):
+        pass
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, L, bits, coeff, vec, out_dir):
+def _worker(rank, world, port, L, bits, coeff, vec, out_dir, exchange="copy"):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         comm = SH.ProcessGroupComm()
-        ham = SH.ShardedHamiltonian(L, bits, coeff, comm, local=_DenseLocal)
+        if exchange == "stage":
+            ham = SH.ShardedHamiltonian(L, bits, coeff, comm, exchange="stage", full=_DenseFull)
+        else:
+            ham = SH.ShardedHamiltonian(L, bits, coeff, comm, local=_DenseLocal)
         x = SH.Shards.split(comm, torch.from_numpy(vec))
         y = SH.Shards.empty_like(x)
         ham.apply(y, x)
@@ -89,8 +112,9 @@ def _worker(rank, world, port, L, bits, coeff, vec, out_dir):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("exchange", ["copy", "stage"])
 @pytest.mark.parametrize("world", [2, 4])
-def test_sharded_apply_over_gloo_ranks(world, tmp_path):
+def test_sharded_apply_over_gloo_ranks(world, exchange, tmp_path):
     L = 8
     bits, coeff = random_terms(L, 60, seed=10 + world)
     # plus terms whose X masks use the top qubits, so every exchange is exercised
@@ -100,7 +124,7 @@ def test_sharded_apply_over_gloo_ranks(world, tmp_path):
     coeff = np.concatenate([coeff, [0.5, -1.25j, 2.0]])
     rng = np.random.default_rng(3)
     vec = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
-    mp.spawn(_worker, args=(world, _free_port(), L, bits, coeff, vec, str(tmp_path)),
+    mp.spawn(_worker, args=(world, _free_port(), L, bits, coeff, vec, str(tmp_path), exchange),
              nprocs=world, join=True)
     y = np.load(tmp_path / "y.npy")
     ref = O.dense_matrix(L, bits, coeff) @ vec
