@@ -55,10 +55,11 @@ typedef struct {
                               bytes when source blocks are served from L2 */
     double smem_bytes;   /* bytes moved through shared memory per apply: one
                             element per term (after splitting complex
-                            coefficients) and output element, plus every
-                            staged source tile */
-    int nreads;          /* source-element reads per output element (terms) */
-    int pad;
+                            coefficients, the fused diagonal counting as one)
+                            and output element, plus every staged source tile */
+    int nreads;          /* source-element reads per output element */
+    int diag_terms;      /* real Z strings summed into the row kernel's per-row
+                          * diagonal factor (0: none, or fewer than 4) */
 } rp_ham_info_t;
 
 /* Statistics of one evolve. */

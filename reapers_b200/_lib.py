@@ -31,7 +31,7 @@ class HamInfo(C.Structure):
                 ("tile_exp", C.c_int), ("ngroups", C.c_int), ("threads", C.c_int),
                 ("stages", C.c_int), ("grid", C.c_int), ("alg_bytes", C.c_double),
                 ("kernel", C.c_int), ("window", C.c_int), ("alg_bytes_dram", C.c_double),
-                ("smem_bytes", C.c_double), ("nreads", C.c_int), ("pad", C.c_int)]
+                ("smem_bytes", C.c_double), ("nreads", C.c_int), ("diag_terms", C.c_int)]
 
 
 class EvolveStats(C.Structure):

@@ -158,7 +158,7 @@ void plan_build(ApplyPlan &plan, int len, int dtype, const uint64_t *bits,
     plan.ngroups = (int)plan.groups.size();
     plan.alg_bytes = (double)(plan.ngroups + 1) * D * (double)elem_size(dtype);
     plan.rows = RowPlan{};
-    if (cfg.allow_rows) rowplan_build(plan.rows, len, dtype, bits, coeff, nterms);
+    if (cfg.allow_rows) rowplan_build(plan.rows, len, dtype, bits, coeff, nterms, false, true);
     if (plan.rows.ok) plan.alg_bytes = plan.rows.alg_bytes_smem;
 }
 

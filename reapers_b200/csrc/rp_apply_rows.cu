@@ -40,7 +40,7 @@ static int log2i(uint64_t v) {
 }
 
 void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
-                   int64_t nterms, bool any_len) {
+                   int64_t nterms, bool any_len, bool fuse_diag) {
     rp = RowPlan{};
     const int esz = dtype == 2 ? 16 : 8;
     const int C = 128 / esz;         // elements per row
@@ -67,7 +67,30 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
         if (cr != 0.0 || ci == 0.0) ts.push_back({x, z, cr, 0});
         if (ci != 0.0) ts.push_back({x, z, ci, 1});
     }
-    if ((int)ts.size() > ROW_MAX_TERMS) return;
+    if (fuse_diag) {
+        const auto real_diag = [](const T &t) { return t.x == 0 && t.kind == 0; };
+        const int nd = (int)std::count_if(ts.begin(), ts.end(), real_diag);
+        if (nd >= ROW_DIAG_MIN) {
+            std::vector<T> d;
+            std::vector<T> rest;
+            for (const T &t : ts) (real_diag(t) ? d : rest).push_back(t);
+            ts.swap(rest);
+            std::stable_sort(d.begin(), d.end(), [C](const T &a, const T &b) {
+                return (a.z & (uint32_t)(C - 1)) < (b.z & (uint32_t)(C - 1));
+            });
+            rp.dstart.assign(C + 1, 0);
+            for (const T &t : d) {
+                rp.diag.push_back({t.z >> logC, (float)t.c, t.c});
+                rp.dstart[(t.z & (uint32_t)(C - 1)) + 1]++;
+            }
+            for (int b = 0; b < C; b++) rp.dstart[b + 1] += rp.dstart[b];
+            rp.ndiag = nd;
+        }
+    }
+    if ((int)ts.size() > ROW_MAX_TERMS || rp.ndiag > ROW_MAX_TERMS) {
+        rp = RowPlan{};
+        return;
+    }
     std::stable_sort(ts.begin(), ts.end(),
                      [B](const T &a, const T &b) { return (a.x >> B) < (b.x >> B); });
     for (size_t k = 0; k < ts.size(); k++) {
@@ -91,6 +114,10 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
         r.cd = ts[k].c;
         rp.terms.push_back(r);
     }
+    // the fused diagonal is applied with group 0, which must then be the
+    // output's own tile (x >> B == 0), with or without terms of its own
+    if (rp.ndiag && (rp.groups.empty() || rp.groups[0].xh != 0))
+        rp.groups.insert(rp.groups.begin(), RowGroup{0u, 0u, 0u, 0u});
     if ((int)rp.groups.size() > ROW_MAX_GROUPS) {
         rp = RowPlan{};
         return;
@@ -125,13 +152,25 @@ void rowplan_upload(RowPlan &rp) {
     RP_CUDA(cudaMalloc((void **)&rp.d_groups, std::max<size_t>(16, rp.groups.size() * sizeof(RowGroup))));
     RP_CUDA(cudaMemcpy(rp.d_groups, rp.groups.data(), rp.groups.size() * sizeof(RowGroup),
                        cudaMemcpyHostToDevice));
+    if (rp.ndiag) {
+        RP_CUDA(cudaMalloc((void **)&rp.d_diag, rp.diag.size() * sizeof(RowDiag)));
+        RP_CUDA(cudaMemcpy(rp.d_diag, rp.diag.data(), rp.diag.size() * sizeof(RowDiag),
+                           cudaMemcpyHostToDevice));
+        RP_CUDA(cudaMalloc((void **)&rp.d_dstart, rp.dstart.size() * sizeof(uint32_t)));
+        RP_CUDA(cudaMemcpy(rp.d_dstart, rp.dstart.data(), rp.dstart.size() * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice));
+    }
 }
 
 void rowplan_free(RowPlan &rp) {
     if (rp.d_terms) cudaFree(rp.d_terms);
     if (rp.d_groups) cudaFree(rp.d_groups);
+    if (rp.d_diag) cudaFree(rp.d_diag);
+    if (rp.d_dstart) cudaFree(rp.d_dstart);
     rp.d_terms = nullptr;
     rp.d_groups = nullptr;
+    rp.d_diag = nullptr;
+    rp.d_dstart = nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -148,6 +187,10 @@ struct RowArgs {
     // source tile s (global) is local tile s & (2^lbits - 1) of map s >> lbits
     uint32_t gtile0;
     int lbits, nmaps;
+    // fused diagonal (DIAG kernels): ndiag real Z strings by in-row bucket
+    const RowDiag *diag;
+    const uint32_t *dstart;
+    int ndiag;
     double alpha;
     const double *alpha_dev;
     int accumulate;
@@ -162,10 +205,63 @@ constexpr int ROW_P = 256;          // consumer threads = rows per tile
 constexpr int ROW_NW = ROW_P / 32;
 constexpr unsigned ROW_TILE_BYTES = 256 * 128;
 
+// The fused diagonal of one output row (index bits above the in-row ones:
+// hi), added to acc: bucket sums a_b = sum_{t: z_t & (C-1) = b} c_t
+// (-1)^popc(zhi_t & hi), then a Walsh-Hadamard transform over the in-row
+// bits gives d(e) = sum_b a_b (-1)^popc(b & e) for every element e, applied
+// to the own row read from the staged tile at rq (no permutation).
+template <typename Real>
+__device__ __forceinline__ void apply_diag(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
+                                           const RowDiag *sdiag, const uint32_t *sdstart, uint32_t hi,
+                                           uint32_t rq) {
+    constexpr int C = 128 / (int)sizeof(Cplx<Real>);
+    Real d[C];
+#pragma unroll
+    for (int b = 0; b < C; b++) {
+        Real sum = Real(0);
+        const uint32_t t1 = sdstart[b + 1];
+        for (uint32_t t = sdstart[b]; t < t1; t++) {
+            const RowDiag dt = sdiag[t];
+            Real c;
+            if constexpr (sizeof(Real) == 4) c = dt.cf;
+            else c = dt.cd;
+            sum += (__popc(dt.zhi & hi) & 1) ? -c : c;
+        }
+        d[b] = sum;
+    }
+#pragma unroll
+    for (int h = 1; h < C; h <<= 1) {
+#pragma unroll
+        for (int e = 0; e < C; e++) {
+            if (!(e & h)) {
+                const Real u = d[e], v = d[e | h];
+                d[e] = u + v;
+                d[e | h] = u - v;
+            }
+        }
+    }
+    float4 w[8];
+    load_row(w, rq);
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        if constexpr (C == 16) {
+            acc[2 * p].x = fma(d[2 * p], w[p].x, acc[2 * p].x);
+            acc[2 * p].y = fma(d[2 * p], w[p].y, acc[2 * p].y);
+            acc[2 * p + 1].x = fma(d[2 * p + 1], w[p].z, acc[2 * p + 1].x);
+            acc[2 * p + 1].y = fma(d[2 * p + 1], w[p].w, acc[2 * p + 1].y);
+        } else {
+            const double vx = __hiloint2double(__float_as_int(w[p].y), __float_as_int(w[p].x));
+            const double vy = __hiloint2double(__float_as_int(w[p].w), __float_as_int(w[p].z));
+            acc[p].x = fma(d[p], vx, acc[p].x);
+            acc[p].y = fma(d[p], vy, acc[p].y);
+        }
+    }
+}
+
 // The row kernel's body.  maps points at kernel-parameter tensor maps: one
 // over the whole input state, or (SHARD) one per input shard, a shard being
 // this GPU's memory or a peer's.
-template <typename Real, bool SHARD>
+template <typename Real, bool SHARD, bool DIAG>
 __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const RowArgs<Real> a) {
     constexpr int C = 128 / (int)sizeof(Cplx<Real>);   // elements per row
     constexpr int LOGC = C == 16 ? 4 : 3;
@@ -178,7 +274,9 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
     unsigned char *stage = smem;
     RowTerm<float> *sterms = reinterpret_cast<RowTerm<float> *>(smem + (size_t)S * ROW_TILE_BYTES);
     RowGroup *sgroups = reinterpret_cast<RowGroup *>(sterms + a.nterms);
-    uint64_t *full = reinterpret_cast<uint64_t *>(sgroups + a.ngroups);
+    RowDiag *sdiag = reinterpret_cast<RowDiag *>(sgroups + a.ngroups);
+    uint32_t *sdstart = reinterpret_cast<uint32_t *>(sdiag + (DIAG ? a.ndiag : 0));
+    uint64_t *full = reinterpret_cast<uint64_t *>(sdstart + (DIAG ? (C + 4) & ~3 : 0));
     uint64_t *empty = full + S;
     double *red = reinterpret_cast<double *>(empty + S);
     __shared__ int s_abort;
@@ -188,6 +286,10 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < a.nterms; i += blockDim.x) sterms[i] = a.terms[i];
     for (int i = tid; i < a.ngroups; i += blockDim.x) sgroups[i] = a.groups[i];
+    if constexpr (DIAG) {
+        for (int i = tid; i < a.ndiag; i += blockDim.x) sdiag[i] = a.diag[i];
+        for (int i = tid; i <= C; i += blockDim.x) sdstart[i] = a.dstart[i];
+    }
     if (a.ndot)
         for (int i = tid; i < ROW_NW * a.ndot * 4; i += blockDim.x) red[i] = 0.0;
     if (tid == 0) {
@@ -279,6 +381,12 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
                         default: chunk_case<Real, 7>(acc, rq, c0, jc); break;
                     }
                 }
+                if constexpr (DIAG) {
+                    // group 0 is the output's own tile: the diagonal factor
+                    // d(u) = sum_t c_t (-1)^popc(z_t & u) times the own row
+                    if (g == 0) apply_diag<Real>(acc, sdiag, sdstart, (og << 8) | row,
+                                                 (tile + row * 128u) | ((row & 7u) << 4));
+                }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[s]);
             }
@@ -367,10 +475,10 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
     }
 }
 
-template <typename Real, int MINB>
+template <typename Real, int MINB, bool DIAG>
 __global__ void __launch_bounds__(ROW_P + 32, MINB)
     k_apply_rows(const __grid_constant__ CUtensorMap tmap, const RowArgs<Real> a) {
-    apply_rows_body<Real, false>(&tmap, a);
+    apply_rows_body<Real, false, DIAG>(&tmap, a);
 }
 
 // One output shard of a state split by its top qubits: the source tiles come
@@ -380,10 +488,10 @@ struct RowShardMaps {
     CUtensorMap m[ROW_MAX_SHARDS];
 };
 
-template <typename Real, int MINB>
+template <typename Real, int MINB, bool DIAG>
 __global__ void __launch_bounds__(ROW_P + 32, MINB)
     k_apply_rows_shard(const __grid_constant__ RowShardMaps maps, const RowArgs<Real> a) {
-    apply_rows_body<Real, true>(maps.m, a);
+    apply_rows_body<Real, true, DIAG>(maps.m, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -430,8 +538,11 @@ CUtensorMap make_row_map(const void *base, int len, int dtype) {
 template <typename Real>
 static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch &l,
                           cudaStream_t st) {
+    const bool diag = rp.ndiag > 0;
+    const int C = 128 / (int)sizeof(Cplx<Real>);
     const size_t fixed = (size_t)rp.nterms * sizeof(RowTerm<float>) +
                          (size_t)rp.groups.size() * sizeof(RowGroup) +
+                         (diag ? (size_t)rp.ndiag * sizeof(RowDiag) + (size_t)((C + 4) & ~3) * 4 : 0) +
                          (size_t)ROW_NW * l.ndot * 4 * sizeof(double) + 1024;
     // CTAs per SM (RPB200_ROW_CTAS, 1 or 2; default 2): the shared memory of
     // an SM (228 KB, 1 KB of it reserved per CTA) is split between them
@@ -445,15 +556,17 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     RP_REQUIRE(S >= 2, -2, "Hamiltonian table too large for the row kernel");
     const size_t smem = (size_t)S * ROW_TILE_BYTES + fixed + (size_t)2 * S * sizeof(uint64_t);
     const bool shard = l.shards != nullptr;
-    auto kern = ctas == 2 ? k_apply_rows<Real, 2> : k_apply_rows<Real, 1>;
-    auto kern_sh = ctas == 2 ? k_apply_rows_shard<Real, 2> : k_apply_rows_shard<Real, 1>;
-    static size_t attr[2][2] = {{0, 0}, {0, 0}};
-    if (smem > attr[shard][ctas - 1]) {
+    auto kern = ctas == 2 ? (diag ? k_apply_rows<Real, 2, true> : k_apply_rows<Real, 2, false>)
+                          : (diag ? k_apply_rows<Real, 1, true> : k_apply_rows<Real, 1, false>);
+    auto kern_sh = ctas == 2 ? (diag ? k_apply_rows_shard<Real, 2, true> : k_apply_rows_shard<Real, 2, false>)
+                             : (diag ? k_apply_rows_shard<Real, 1, true> : k_apply_rows_shard<Real, 1, false>);
+    static size_t attr[2][2][2] = {};
+    if (smem > attr[shard][diag][ctas - 1]) {
         if (shard)
             RP_CUDA(cudaFuncSetAttribute(kern_sh, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         else
             RP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr[shard][ctas - 1] = smem;
+        attr[shard][diag][ctas - 1] = smem;
     }
     const int lbits = shard ? ilog2((uint32_t)rp.ntiles) - l.shard_bits : 0;
     const int local_tiles = shard ? rp.ntiles >> l.shard_bits : rp.ntiles;
@@ -468,6 +581,9 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     a.gtile0 = shard ? (uint32_t)l.shard_rank << lbits : 0u;
     a.lbits = lbits;
     a.nmaps = shard ? 1 << l.shard_bits : 1;
+    a.diag = rp.d_diag;
+    a.dstart = rp.d_dstart;
+    a.ndiag = rp.ndiag;
     a.stages = S;
     a.alpha = l.alpha;
     a.alpha_dev = l.alpha_dev;

@@ -30,6 +30,16 @@ struct alignas(16) RowGroup {
     uint32_t xh, first, count, pad;
 };
 
+// A real-coefficient Z string (X mask 0) folded into the per-row diagonal
+// factor: zhi = z >> logC, the Z bits above the in-row element bits; the
+// terms are bucketed by z & (C - 1), their in-row Z bits.
+struct alignas(16) RowDiag {
+    uint32_t zhi;
+    float cf;      // coefficient, FP32 kernels
+    double cd;     // coefficient, FP64 kernels
+};
+static_assert(sizeof(RowDiag) == 16, "layout");
+
 struct RowPlan {
     bool ok = false;          // the row kernel applies to this Hamiltonian
     int B = 0, logC = 0;      // tile exponent, log2(elements per row)
@@ -39,6 +49,13 @@ struct RowPlan {
     std::vector<RowGroup> groups;
     void *d_terms = nullptr;
     RowGroup *d_groups = nullptr;
+    // fused diagonal: real Z strings summed per row (group 0 is then the
+    // source tile x >> B == 0, the output's own tile)
+    int ndiag = 0;
+    std::vector<RowDiag> diag;          // by bucket z & (C - 1)
+    std::vector<uint32_t> dstart;       // C + 1 bucket offsets into diag
+    RowDiag *d_diag = nullptr;
+    uint32_t *d_dstart = nullptr;
     int window = 0;           // CTAs of an aligned tile window (grid size)
     double alg_bytes_smem = 0;  // (G + 1) D s, G = distinct x >> B
     double alg_bytes_dram = 0;  // (G_w + 1) D s, G_w = distinct x >> (B + log2 window)
@@ -48,11 +65,14 @@ struct RowPlan {
 // in shared memory.
 constexpr int ROW_MAX_TERMS = 2048;
 constexpr int ROW_MAX_GROUPS = 1024;
+// Fewest real Z strings worth the fused diagonal (below it they stay terms).
+constexpr int ROW_DIAG_MIN = 4;
 
 // any_len: build the table for any len >= the tile exponent (the batched
-// kernel); otherwise only for states of at least 128 tiles.
+// kernel); otherwise only for states of at least 128 tiles.  fuse_diag: fold
+// the real Z strings into the per-row diagonal factor (single-state kernel).
 void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const double *coeff,
-                   int64_t nterms, bool any_len = false);
+                   int64_t nterms, bool any_len = false, bool fuse_diag = false);
 void rowplan_upload(RowPlan &rp);
 void rowplan_free(RowPlan &rp);
 

@@ -326,14 +326,15 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info) {
         const double vbytes = std::ldexp(1.0, p.len) * (p.dtype == RP_C128 ? 16.0 : 8.0);
         const int nt = p.rows.ok ? p.rows.nterms : p.nterms;
         const int ng = p.rows.ok ? (int)p.rows.groups.size() : p.ngroups;
-        info->nreads = nt;
-        info->smem_bytes = (double)(nt + ng) * vbytes;
-        info->pad = 0;
+        const int nd = p.rows.ok ? p.rows.ndiag : 0;
+        info->nreads = nt + (nd ? 1 : 0);
+        info->smem_bytes = (double)(nt + ng + (nd ? 1 : 0)) * vbytes;
+        info->diag_terms = nd;
         if (p.rows.ok) {
             info->tile_exp = p.rows.B;
             info->ngroups = (int)p.rows.groups.size();
             info->threads = 256;
-            info->nterms = p.rows.nterms;
+            info->nterms = p.rows.nterms + p.rows.ndiag;
         }
     });
 }

@@ -18,6 +18,16 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// The 128-byte row at shared address rq, chunk p from rq ^ (p << 4).
+__device__ __forceinline__ void load_row(float4 (&w)[8], uint32_t rq) {
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                     : "=f"(w[p].x), "=f"(w[p].y), "=f"(w[p].z), "=f"(w[p].w)
+                     : "r"(rq ^ ((uint32_t)p << 4)));
+    }
+}
+
 // One term over a whole row.  w[p], loaded from rq ^ (p << 4), holds source
 // chunk p ^ xq (the permutation is in the address); case K = x0 | z0 << 1 | kind << 2.  Output
 // element u = EPC p + e takes source element e ^ x0 of w[p] with sign

@@ -369,3 +369,63 @@ def test_apply_randomised_sweep(cuda, case):
     assert relerr(got, ref) < tol, (L, dtype, kinds, len(bits), ham.info()["kernel"])
     ham.apply(out, x, accumulate=True)
     assert relerr(out.cpu().numpy().astype(np.complex128), 2 * ref) < tol
+
+
+def _diag_heavy(rng, L):
+    """Real Z strings on in-row and high qubits (fused into the diagonal
+    factor), an imaginary one and a complex one (its imaginary part stays a
+    term), plus X terms on low and high qubits."""
+    def zbit(i):
+        return 1 << (2 * i + 1)
+
+    def xbit(i):
+        return 1 << (2 * i)
+
+    bits, coeff = [], []
+    for i in range(L):                      # fields, every qubit
+        bits.append(zbit(i))
+        coeff.append(rng.uniform(-1, 1))
+    for i in range(L - 1):                  # ZZ couplings
+        bits.append(zbit(i) | zbit(i + 1))
+        coeff.append(rng.uniform(-1, 1))
+    bits.append(zbit(0) | zbit(3) | zbit(L - 1))
+    coeff.append(0.3j)                      # imaginary diagonal: a plain term
+    bits.append(zbit(1) | zbit(L - 2))
+    coeff.append(0.2 - 0.4j)                # complex diagonal: split
+    for i in (0, 2, 5, L - 3, L - 1):       # X and Y terms, low and high
+        bits.append(xbit(i))
+        coeff.append(rng.uniform(-1, 1))
+        bits.append(xbit(i) | zbit(i))
+        coeff.append(1j * rng.uniform(-1, 1))
+    return np.array(bits, dtype=np.uint64), np.array(coeff, dtype=np.complex128)
+
+
+@pytest.mark.parametrize("dtype,L", [("c64", 19), ("c64", 21), ("c128", 18), ("c128", 20)])
+@pytest.mark.parametrize("model", ["diag_heavy", "xxz", "fields_only"])
+def test_row_kernel_fused_diagonal(cuda, dtype, L, model):
+    """Real Z strings summed per row into one diagonal factor (bucketed by
+    their in-row Z bits, Walsh-Hadamard over those bits) against the oracle,
+    overwrite and accumulate; "fields_only" has no other terms on the
+    output's own tile, so the kernel's tile group 0 holds the diagonal alone."""
+    rng = np.random.default_rng(L)
+    if model == "diag_heavy":
+        bits, coeff = _diag_heavy(rng, L)
+    elif model == "xxz":
+        bits, coeff = rb.syk.xxz_chain(L, 0.8, rng.uniform(-1, 1, L), periodic=True)
+    else:
+        bits = np.array([1 << (2 * i + 1) for i in range(L)] + [1 << (2 * (L - 1))],
+                        dtype=np.uint64)
+        coeff = np.concatenate([rng.uniform(-1, 1, L), [0.7]]).astype(np.complex128)
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    info = ham.info()
+    assert info["kernel"] == 2 and info["diag_terms"] >= 4, info
+    v = rand_vec(rng, L)
+    x = to_dev(v, dtype)
+    out = torch.empty_like(x)
+    ham.apply(out, x)
+    ref = O.apply(L, bits, coeff, v)
+    tol = FP64_TOL if dtype == "c128" else FP32_TOL
+    assert relerr(out.cpu().numpy().astype(np.complex128), ref) < tol
+    ham.apply(out, x, accumulate=True)
+    assert relerr(out.cpu().numpy().astype(np.complex128), 2 * ref) < tol
+    ham.close()
