@@ -619,6 +619,10 @@ def run_ours(args):
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
+    # the sharded leg uses this leg's Hamiltonian and state, so it runs
+    # before the OTOC leg frees them
+    if legs and args.config == "syk56" and not args.no_shard:
+        line["sharded_peer_syk56"] = shard_leg(ham, x, L)
     if legs and args.config == "syk56" and not args.no_otoc:
         del x, ham
         torch.cuda.empty_cache()
@@ -629,8 +633,6 @@ def run_ours(args):
         line["otoc_batched_syk32_40"] = batch_leg(seed=rank)
     if legs and args.config == "syk56" and not args.no_steps:
         line["learned_steps"] = step_leg(seed=rank)
-    if legs and args.config == "syk56" and not args.no_shard:
-        line["sharded_peer_syk56"] = shard_leg(ham, x, L)
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
