@@ -122,7 +122,7 @@ class Hamiltonian:
         _lib.call("rp_apply_host", self._h, n, ip, op)
         return outs
 
-    def apply_shard(self, out, shards, accumulate=False, rank=None):
+    def apply_shard(self, out, shards, rank, accumulate=False):
         """out = output shard `rank` of H applied to the state whose 2^k
         shards (top k qubits, k = log2 len(shards)) are the device tensors or
         raw device pointers `shards`; a shard may be a peer's memory (see
@@ -132,7 +132,7 @@ class Hamiltonian:
         k = n.bit_length() - 1
         if n < 2 or 1 << k != n:
             raise ValueError("the number of shards must be a power of two, at least 2")
-        if rank is None or not 0 <= rank < n:
+        if not 0 <= rank < n:
             raise ValueError("rank must name one of the shards")
         want = 1 << (self.len - k)
         if _tcode(out) != self.dtype or out.numel() != want:
