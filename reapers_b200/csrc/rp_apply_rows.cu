@@ -20,6 +20,18 @@
 // groups sharing the high bits of xh read overlapping source blocks back to
 // back from L2.  Two CTAs per SM (2 x 148 = 296 CTAs) give 16 consumer warps
 // per SM to hide shared-memory and FMA latency.
+//
+// Fused diagonal (DIAG variants, Hamiltonians with at least ROW_DIAG_MIN
+// real Z strings): those terms leave the term list; with group 0 (the
+// output's own tile) every row sums their coefficients, signed by its high
+// index bits, into one bucket per in-row Z pattern, and a Walsh-Hadamard
+// transform over the in-row bits gives each element's diagonal factor,
+// applied once to the own row.
+//
+// Sharded variant (k_apply_rows_shard): one output shard of a state split by
+// its top qubits, with one tensor map per input shard; each source tile is
+// loaded from the shard holding it (this GPU's memory or a peer's), the Z
+// signs use the global tile index.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
