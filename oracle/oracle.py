@@ -117,6 +117,24 @@ def syk_terms(N, quartets, couplings):
     return bits, coeff.view(np.complex128)
 
 
+def apply_at(bits, coeff, idx, fetch):
+    """(H vec)[i] for the output indices idx only: the sum of or_apply
+    (inc/cpuimpl.h:747-753 with SpinOp::apply, inc/ops.h:421-440),
+    out[i] = sum_k c_k (-1)^popc(z_k & (i ^ x_k)) vec[i ^ x_k] in list order,
+    with fetch(j) returning vec at the int64 index array j as complex128 --
+    spot checks of states too large for the CPU apply."""
+    x, z = split_bits(bits)
+    idx = np.asarray(idx, dtype=np.uint64)
+    c = np.asarray(coeff, dtype=np.complex128)
+    src = idx[:, None] ^ x[None, :]
+    minus = (np.bitwise_count(z[None, :] & src) & np.uint8(1)).astype(bool)
+    vals = np.asarray(fetch(src.reshape(-1).astype(np.int64)), dtype=np.complex128).reshape(src.shape)
+    out = np.zeros(idx.shape[0], dtype=np.complex128)
+    for k in range(c.shape[0]):
+        out += np.where(minus[:, k], -c[k], c[k]) * vals[:, k]
+    return out
+
+
 def apply(length, bits, coeff, vec, out=None):
     """H.vec, complex128 in and out."""
     bits = np.ascontiguousarray(bits, dtype=np.uint64)
