@@ -103,12 +103,22 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
         rp = RowPlan{};
         return;
     }
-    std::stable_sort(ts.begin(), ts.end(),
-                     [B](const T &a, const T &b) { return (a.x >> B) < (b.x >> B); });
+    // by source tile (x >> B); in fused-diagonal (spin-chain) plans also by
+    // the full X mask, so that terms reading the same source row with the
+    // same case are adjacent and share one row load (ROW_SAME_SRC)
+    const bool runs = rp.ndiag > 0;
+    std::stable_sort(ts.begin(), ts.end(), [B, runs](const T &a, const T &b) {
+        if ((a.x >> B) != (b.x >> B)) return (a.x >> B) < (b.x >> B);
+        return runs && a.x < b.x;
+    });
     for (size_t k = 0; k < ts.size(); k++) {
         const uint32_t xh = ts[k].x >> B;
+        bool same = false;
         if (rp.groups.empty() || rp.groups.back().xh != xh)
             rp.groups.push_back({xh, (uint32_t)k, 0u, 0u});
+        else
+            same = runs && ts[k].x == ts[k - 1].x && ts[k].kind == ts[k - 1].kind &&
+                   ((ts[k].z ^ ts[k - 1].z) & (uint32_t)(EPC - 1)) == 0;
         rp.groups.back().count++;
         const uint32_t xl = ts[k].x & ((1u << B) - 1);
         const uint32_t xr = xl >> logC, xc = xl & (uint32_t)(C - 1);
@@ -119,7 +129,8 @@ void rowplan_build(RowPlan &rp, int len, int dtype, const uint64_t *bits, const 
         uint32_t jc = 0;
         for (int p = 0; p < 8; p++) jc |= (uint32_t)(__builtin_popcount(zq & (p ^ xq)) & 1) << p;
         RowTerm<float> r{};
-        r.cs = xr | (xq << 8) | ((x0 | (z0 << 1) | ((uint32_t)ts[k].kind << 2)) << 11);
+        r.cs = xr | (xq << 8) | ((x0 | (z0 << 1) | ((uint32_t)ts[k].kind << 2)) << 11) |
+               (same ? ROW_SAME_SRC : 0u);
         r.z = ts[k].z;
         r.js = jc;
         r.cf = (float)ts[k].c;
@@ -369,28 +380,73 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
                     break;
                 }
                 const uint32_t tile = smem_u32(stage + (size_t)s * ROW_TILE_BYTES);
-                for (uint32_t k = gd.first; k < gd.first + gd.count; ++k) {
-                    const uint4 d0 = *reinterpret_cast<const uint4 *>(&sterms[k]);
-                    const uint32_t cs = d0.x, z = d0.y, jc = d0.z;
-                    const uint32_t sr = row ^ (cs & 0xFFu);
-                    const uint32_t xq = (cs >> 8) & 7u;
-                    const uint32_t s0 = (uint32_t)(__popc(z & (src_hi | (sr << LOGC))) & 1);
-                    Real c0;
-                    if constexpr (sizeof(Real) == 4) c0 = __uint_as_float(d0.w);
-                    else c0 = sterms[k].cd;
-                    if (s0) c0 = -c0;
-                    // chunk p of the permuted source row sits at physical
-                    // chunk p ^ xq ^ (sr & 7) of row sr
-                    const uint32_t rq = (tile + sr * 128u) | ((xq ^ (sr & 7u)) << 4);
-                    switch ((cs >> 11) & 7u) {
-                        case 0: chunk_case<Real, 0>(acc, rq, c0, jc); break;
-                        case 1: chunk_case<Real, 1>(acc, rq, c0, jc); break;
-                        case 2: chunk_case<Real, 2>(acc, rq, c0, jc); break;
-                        case 3: chunk_case<Real, 3>(acc, rq, c0, jc); break;
-                        case 4: chunk_case<Real, 4>(acc, rq, c0, jc); break;
-                        case 5: chunk_case<Real, 5>(acc, rq, c0, jc); break;
-                        case 6: chunk_case<Real, 6>(acc, rq, c0, jc); break;
-                        default: chunk_case<Real, 7>(acc, rq, c0, jc); break;
+                if constexpr (DIAG) {
+                    // spin-chain plans: consecutive terms with the same X mask
+                    // and case (ROW_SAME_SRC) share one load of their source row
+                    auto decode = [&](uint32_t k, uint32_t &cs, uint32_t &jc, Real &c0) {
+                        const uint4 d0 = *reinterpret_cast<const uint4 *>(&sterms[k]);
+                        cs = d0.x;
+                        jc = d0.z;
+                        const uint32_t sr = row ^ (cs & 0xFFu);
+                        const uint32_t s0 = (uint32_t)(__popc(d0.y & (src_hi | (sr << LOGC))) & 1);
+                        if constexpr (sizeof(Real) == 4) c0 = __uint_as_float(d0.w);
+                        else c0 = sterms[k].cd;
+                        if (s0) c0 = -c0;
+                    };
+                    const uint32_t kend = gd.first + gd.count;
+                    for (uint32_t k = gd.first; k < kend; ++k) {
+                        uint32_t cs, jc;
+                        Real c0;
+                        decode(k, cs, jc, c0);
+                        const uint32_t sr = row ^ (cs & 0xFFu);
+                        const uint32_t xq = (cs >> 8) & 7u;
+                        float4 w[8];
+                        load_row(w, (tile + sr * 128u) | ((xq ^ (sr & 7u)) << 4));
+                        switch ((cs >> 11) & 7u) {
+#define RP_ROW_RUN(K)                                                          \
+    case K:                                                                    \
+        for (;;) {                                                             \
+            row_case<Real, K>(acc, w, c0, jc);                                 \
+            if (k + 1 >= kend || !(sterms[k + 1].cs & ROW_SAME_SRC)) break;    \
+            ++k;                                                               \
+            decode(k, cs, jc, c0);                                             \
+        }                                                                      \
+        break;
+                            RP_ROW_RUN(0)
+                            RP_ROW_RUN(1)
+                            RP_ROW_RUN(2)
+                            RP_ROW_RUN(3)
+                            RP_ROW_RUN(4)
+                            RP_ROW_RUN(5)
+                            RP_ROW_RUN(6)
+                            RP_ROW_RUN(7)
+#undef RP_ROW_RUN
+                        }
+                    }
+                } else {
+                    for (uint32_t k = gd.first; k < gd.first + gd.count; ++k) {
+                        const uint4 d0 = *reinterpret_cast<const uint4 *>(&sterms[k]);
+                        const uint32_t cs = d0.x, z = d0.y, jc = d0.z;
+                        const uint32_t sr = row ^ (cs & 0xFFu);
+                        const uint32_t xq = (cs >> 8) & 7u;
+                        const uint32_t s0 = (uint32_t)(__popc(z & (src_hi | (sr << LOGC))) & 1);
+                        Real c0;
+                        if constexpr (sizeof(Real) == 4) c0 = __uint_as_float(d0.w);
+                        else c0 = sterms[k].cd;
+                        if (s0) c0 = -c0;
+                        // chunk p of the permuted source row sits at physical
+                        // chunk p ^ xq ^ (sr & 7) of row sr
+                        const uint32_t rq = (tile + sr * 128u) | ((xq ^ (sr & 7u)) << 4);
+                        switch ((cs >> 11) & 7u) {
+                            case 0: chunk_case<Real, 0>(acc, rq, c0, jc); break;
+                            case 1: chunk_case<Real, 1>(acc, rq, c0, jc); break;
+                            case 2: chunk_case<Real, 2>(acc, rq, c0, jc); break;
+                            case 3: chunk_case<Real, 3>(acc, rq, c0, jc); break;
+                            case 4: chunk_case<Real, 4>(acc, rq, c0, jc); break;
+                            case 5: chunk_case<Real, 5>(acc, rq, c0, jc); break;
+                            case 6: chunk_case<Real, 6>(acc, rq, c0, jc); break;
+                            default: chunk_case<Real, 7>(acc, rq, c0, jc); break;
+                        }
                     }
                 }
                 if constexpr (DIAG) {

@@ -67,6 +67,10 @@ constexpr int ROW_MAX_TERMS = 2048;
 constexpr int ROW_MAX_GROUPS = 1024;
 // Fewest real Z strings worth the fused diagonal (below it they stay terms).
 constexpr int ROW_DIAG_MIN = 4;
+// RowTerm::cs bit (fused-diagonal plans): this term has the previous term's
+// full X mask and case (bits 0-7 source row offset, 8-10 chunk permutation,
+// 11-13 case), so it is applied to the row already loaded for that term.
+constexpr uint32_t ROW_SAME_SRC = 1u << 14;
 
 // any_len: build the table for any len >= the tile exponent (the batched
 // kernel); otherwise only for states of at least 128 tiles.  fuse_diag: fold

@@ -28,26 +28,19 @@ __device__ __forceinline__ void load_row(float4 (&w)[8], uint32_t rq) {
     }
 }
 
-// One term over a whole row.  w[p], loaded from rq ^ (p << 4), holds source
-// chunk p ^ xq (the permutation is in the address); case K = x0 | z0 << 1 | kind << 2.  Output
-// element u = EPC p + e takes source element e ^ x0 of w[p] with sign
+// One term over a whole row already loaded by load_row.  w[p] holds source
+// chunk p ^ xq (the permutation is in the load address); case K = x0 | z0 << 1 | kind << 2.
+// Output element u = EPC p + e takes source element e ^ x0 of w[p] with sign
 // (chunk sign p) * (-1)^(z0 & (e ^ x0)).
 template <typename Real, int K>
-__device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
-                                           uint32_t rq, Real c0, uint32_t jc) {
+__device__ __forceinline__ void row_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
+                                         const float4 (&w)[8], Real c0, uint32_t jc) {
     constexpr int EPC = 16 / (int)sizeof(Cplx<Real>);
     constexpr int X0 = K & 1, Z0 = (K >> 1) & 1, KIND = K >> 2;
     if constexpr (EPC == 1 && (X0 || Z0)) {
         return;
     } else {
         const Real cn = -c0;
-        float4 w[8];
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(w[p].x), "=f"(w[p].y), "=f"(w[p].z), "=f"(w[p].w)
-                         : "r"(rq ^ ((uint32_t)p << 4)));
-        }
 #pragma unroll
         for (int p = 0; p < 8; p++) {
             const Real cp = ((jc >> p) & 1u) ? cn : c0;
@@ -73,6 +66,21 @@ __device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<R
                 }
             }
         }
+    }
+}
+
+// One term over a whole row: its source row from rq (see load_row), then
+// the case.
+template <typename Real, int K>
+__device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
+                                           uint32_t rq, Real c0, uint32_t jc) {
+    constexpr int EPC = 16 / (int)sizeof(Cplx<Real>);
+    if constexpr (EPC == 1 && ((K & 1) || ((K >> 1) & 1))) {
+        return;
+    } else {
+        float4 w[8];
+        load_row(w, rq);
+        row_case<Real, K>(acc, w, c0, jc);
     }
 }
 
