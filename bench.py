@@ -304,6 +304,41 @@ def shard_leg(ham, x, L, reps=3):
     return out
 
 
+def xxz_leg(clocks=None, L=28, reps=10):
+    """H.psi on the XXZ chain (open, J = Jz = 1, fields U[-0.5, 0.5], 2^28
+    complex64): the row kernel's spin-chain variant (real Z strings summed
+    into one per-row diagonal factor, terms with the same X mask sharing a
+    row load), with its compulsory-DRAM and shared-memory fractions."""
+    import torch
+    import reapers_b200 as rb
+    bits, coeff = rb.syk.xxz_chain(L, 1.0, np.random.default_rng(1).uniform(-0.5, 0.5, L))
+    ham = rb.Hamiltonian(L, bits, coeff, "c64")
+    info = ham.info()
+    x = rb.random_state(L, "c64", seed=3)
+    y = torch.empty_like(x)
+    st = rb.stream()
+    for _ in range(3):
+        ham.apply(y, x)
+    rb.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        ham.apply(y, x)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    peak, _ = measured_peak()
+    dram = info["alg_bytes_dram"] / t / 1e9
+    out = {"workload": f"XXZ chain L={L} (2^{L} complex64), open, fields U[-0.5, 0.5]",
+           "terms": info["nterms"], "diag_terms": info["diag_terms"], "ms": round(t * 1e3, 4),
+           "compulsory_dram_GBps": round(dram, 1), "dram_frac": round(dram / peak, 4),
+           "on_chip": on_chip_bound(info, L, {"dtype": "c64"}, t, clocks)}
+    del x, y
+    ham.close()
+    return out
+
+
 def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
               seq_per_size=2, tune=True):
     """Batched OTOC sample: nreal disorder realisations x nstates random
@@ -619,6 +654,8 @@ def run_ours(args):
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
+    if legs and args.config == "syk56" and not args.no_xxz:
+        line["hpsi_xxz28"] = xxz_leg(clocks)
     # the sharded leg uses this leg's Hamiltonian and state, so it runs
     # before the OTOC leg frees them
     if legs and args.config == "syk56" and not args.no_shard:
@@ -708,6 +745,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="syk56")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-xxz", action="store_true", help="skip the XXZ chain H.psi leg")
     ap.add_argument("--no-shard", action="store_true",
                     help="skip the peer-read sharded H.psi leg (virtual shards on one GPU)")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")

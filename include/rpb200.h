@@ -54,10 +54,12 @@ typedef struct {
                               x >> (tile_exp + log2 window): the compulsory DRAM
                               bytes when source blocks are served from L2 */
     double smem_bytes;   /* bytes moved through shared memory per apply: one
-                            element per term (after splitting complex
-                            coefficients, the fused diagonal counting as one)
-                            and output element, plus every staged source tile */
-    int nreads;          /* source-element reads per output element */
+                            element per source-row load (a term after
+                            splitting complex coefficients, less the terms
+                            that reuse the previous term's row, the fused
+                            diagonal counting as one) and output element,
+                            plus every staged source tile */
+    int nreads;          /* source-row loads per output element */
     int diag_terms;      /* real Z strings summed into the row kernel's per-row
                           * diagonal factor (0: none, or fewer than 4) */
 } rp_ham_info_t;

@@ -327,8 +327,13 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info) {
         const int nt = p.rows.ok ? p.rows.nterms : p.nterms;
         const int ng = p.rows.ok ? (int)p.rows.groups.size() : p.ngroups;
         const int nd = p.rows.ok ? p.rows.ndiag : 0;
-        info->nreads = nt + (nd ? 1 : 0);
-        info->smem_bytes = (double)(nt + ng + (nd ? 1 : 0)) * vbytes;
+        // row loads per output element: terms that reuse the previous term's
+        // row (ROW_SAME_SRC) load none; the fused diagonal loads the own row
+        int shared = 0;
+        if (p.rows.ok)
+            for (const auto &t : p.rows.terms) shared += (t.cs & ROW_SAME_SRC) ? 1 : 0;
+        info->nreads = nt - shared + (nd ? 1 : 0);
+        info->smem_bytes = (double)(info->nreads + ng) * vbytes;
         info->diag_terms = nd;
         if (p.rows.ok) {
             info->tile_exp = p.rows.B;
