@@ -217,3 +217,26 @@ def test_peer_apply_across_processes_through_ipc(rb):
     for p in procs:
         p.join(timeout=60)
     assert all(ok for _, ok, _ in res), res
+
+
+def test_ipc_entry_points_reject_bad_arguments(rb):
+    import ctypes as C
+    from reapers_b200 import _lib
+    lib = _lib.load()
+    # a pointer this process never opened
+    rc = lib.rp_ipc_close(C.c_void_p(0x1000))
+    assert rc == -2 and "not opened by rp_ipc_open" in lib.rp_last_error().decode()
+    # host memory is not a device allocation
+    host = (C.c_char * 64)()
+    h = _lib.IpcHandle()
+    rc = lib.rp_ipc_export(C.cast(host, C.c_void_p), C.byref(h))
+    assert rc == -2 and "not a device allocation" in lib.rp_last_error().decode()
+    assert lib.rp_ipc_export(None, C.byref(h)) == -2
+    assert lib.rp_ipc_open(None, C.byref(C.c_void_p())) == -2
+    # a device tensor exports: the handle names its allocation, the offset
+    # its place inside it
+    t = torch.empty(1 << 20, dtype=torch.complex64, device="cuda")
+    view = t[4096:]
+    data, off0 = rb.ipc_export(t)
+    data2, off1 = rb.ipc_export(view)
+    assert data == data2 and off1 - off0 == 4096 * 8
