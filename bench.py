@@ -304,38 +304,52 @@ def shard_leg(ham, x, L, reps=3):
     return out
 
 
-def xxz_leg(clocks=None, L=28, reps=10):
-    """H.psi on the XXZ chain (open, J = Jz = 1, fields U[-0.5, 0.5], 2^28
-    complex64): the row kernel's spin-chain variant (real Z strings summed
-    into one per-row diagonal factor, terms with the same X mask sharing a
-    row load), with its compulsory-DRAM and shared-memory fractions."""
+def _tfim_chain(L, J=1.0, h=0.7):
+    """Transverse-field Ising chain: J Z_i Z_{i+1} (open) + h X_i."""
+    bits = [(1 << (2 * i + 1)) | (1 << (2 * i + 3)) for i in range(L - 1)]
+    bits += [1 << (2 * i) for i in range(L)]
+    coeff = [J] * (L - 1) + [h] * L
+    return np.array(bits, dtype=np.uint64), np.array(coeff, dtype=np.complex128)
+
+
+def spin_chain_leg(clocks=None, L=28, reps=10):
+    """H.psi on two spin chains of 2^28 complex64 elements -- the XXZ chain
+    (open, J = Jz = 1, fields U[-0.5, 0.5]) and the transverse-field Ising
+    chain (J = 1, h = 0.7) -- on the row kernel's spin-chain variant (real Z
+    strings summed into one per-row diagonal factor, terms with the same X
+    mask sharing a row load), with the compulsory-DRAM and shared-memory
+    fractions: where the kernel moves from shared-memory bound to HBM bound."""
     import torch
     import reapers_b200 as rb
-    bits, coeff = rb.syk.xxz_chain(L, 1.0, np.random.default_rng(1).uniform(-0.5, 0.5, L))
-    ham = rb.Hamiltonian(L, bits, coeff, "c64")
-    info = ham.info()
+    peak, _ = measured_peak()
+    st = rb.stream()
+    models = {"xxz": rb.syk.xxz_chain(L, 1.0, np.random.default_rng(1).uniform(-0.5, 0.5, L)),
+              "tfim": _tfim_chain(L)}
+    out = {"workload": f"spin chains of L={L} (2^{L} complex64): XXZ (open, fields U[-0.5, 0.5]), "
+                       f"transverse-field Ising (J=1, h=0.7)"}
     x = rb.random_state(L, "c64", seed=3)
     y = torch.empty_like(x)
-    st = rb.stream()
-    for _ in range(3):
-        ham.apply(y, x)
-    rb.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(reps):
-        ham.apply(y, x)
-    e1.record(st)
-    e1.synchronize()
-    t = e0.elapsed_time(e1) / 1e3 / reps
-    peak, _ = measured_peak()
-    dram = info["alg_bytes_dram"] / t / 1e9
-    out = {"workload": f"XXZ chain L={L} (2^{L} complex64), open, fields U[-0.5, 0.5]",
-           "terms": info["nterms"], "diag_terms": info["diag_terms"], "ms": round(t * 1e3, 4),
-           "compulsory_dram_GBps": round(dram, 1), "dram_frac": round(dram / peak, 4),
-           "on_chip": on_chip_bound(info, L, {"dtype": "c64"}, t, clocks)}
+    for name, (bits, coeff) in models.items():
+        ham = rb.Hamiltonian(L, bits, coeff, "c64")
+        info = ham.info()
+        for _ in range(3):
+            ham.apply(y, x)
+        rb.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            ham.apply(y, x)
+        e1.record(st)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        dram = info["alg_bytes_dram"] / t / 1e9
+        out[name] = {"terms": info["nterms"], "diag_terms": info["diag_terms"],
+                     "source_tile_groups": info["ngroups"], "ms": round(t * 1e3, 4),
+                     "compulsory_dram_GBps": round(dram, 1), "dram_frac": round(dram / peak, 4),
+                     "on_chip": on_chip_bound(info, L, {"dtype": "c64"}, t, clocks)}
+        ham.close()
     del x, y
-    ham.close()
     return out
 
 
@@ -654,8 +668,8 @@ def run_ours(args):
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
-    if legs and args.config == "syk56" and not args.no_xxz:
-        line["hpsi_xxz28"] = xxz_leg(clocks)
+    if legs and args.config == "syk56" and not args.no_chains:
+        line["hpsi_spin_chains_l28"] = spin_chain_leg(clocks)
     # the sharded leg uses this leg's Hamiltonian and state, so it runs
     # before the OTOC leg frees them
     if legs and args.config == "syk56" and not args.no_shard:
@@ -745,7 +759,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="syk56")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--no-xxz", action="store_true", help="skip the XXZ chain H.psi leg")
+    ap.add_argument("--no-chains", action="store_true",
+                    help="skip the spin-chain H.psi leg (XXZ, transverse-field Ising)")
     ap.add_argument("--no-shard", action="store_true",
                     help="skip the peer-read sharded H.psi leg (virtual shards on one GPU)")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
