@@ -6,11 +6,13 @@ Workload (default, ``--config syk56``): sparse SYK with N = 56 Majoranas on
 H.psi in FP32.  ``--config syk48``: sparse SYK N = 48 (24 qubits), 384 terms, FP64.
 
 A step is one H.psi product over the whole state.  The metric is H.psi HBM
-GB/s: the algorithmic bytes of one apply, (G + 1) * 2^L * sizeof(element)
-with G the number of distinct source tiles per output tile (every distinct
-tile read once per output tile, plus the write), divided by the device time
-of the kernel.  Inputs are larger than L2 (2 GiB vs 126 MB), so no flush is
-needed between steps.
+GB/s: the compulsory DRAM bytes of one apply, (G_w + 1) * 2^L *
+sizeof(element), divided by the device time of the kernel.  G_w is the number
+of distinct source blocks per block of output tiles in flight (the kernel's
+window of 296 tiles of 2^12 elements: distinct x >> 20 for the N = 56
+Hamiltonian); every such source block must come from HBM once per window and
+the output is written once.  Inputs are larger than L2 (2 GiB vs 126 MB), so
+no flush is needed between steps.
 
 Multi-GPU (torchrun): every rank runs an independent replica (its own
 disorder realisation); no collective on the data path ("replicas only");
@@ -19,7 +21,8 @@ the value is the sum over ranks of bytes / the max over ranks of time.
 ``--impl reference`` times the reference's own CPU implementation
 (oracle/_ref/ref_driver: SpinOp::apply in CPUImpl::apply_ops's loop, OpenMP
 over all host threads) on a bounded slice of output rows of the same
-workload, in the same unit.
+workload, in the same unit: the bytes of the whole apply scaled by the
+fraction of rows computed, i.e. a rate extrapolated from the row sample.
 """
 from __future__ import annotations
 
@@ -141,20 +144,22 @@ def on_chip_bound(info, L, cfg, t_step, clocks):
             "frac": round(ach / peak, 4)}
 
 
-def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
+def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16, last=True):
     """N = 56 OTOC F(t) = <psi0| W(t) V W(t) V |psi0> (W = b_{N-1}, V = b_{N-2},
     the operators of examples/simple-syk-krylov.cc) on a bounded sample of the
-    20-point time grid on [0, 15] (t = 0 and the first `npts` points), one
+    20-point time grid on [0, 15] (t = 0, the first `npts` points and, with
+    `last`, the final point t = 15, where the evolves restart most), one
     disorder realisation x one state, m = 16, for the plain FP64 path
     (reference default tol = FP64 epsilon) and the mixed path (FP32 vectors
     and H.psi, FP64 inner products / Hessenberg / expm, tol = FP32 epsilon).
-    Error: max |F_mixed - F_fp64| / |F_fp64(0)| over the sampled points."""
+    Error: max |F_mixed - F_fp64| / |F_fp64(0)| over the sampled points, and
+    per point; time and H.psi count per point."""
     import torch
     import reapers_b200 as rb
     L = cfg["N"] // 2
     N = cfg["N"]
     grid = np.linspace(0.0, 15.0, 20)
-    times = [0.0] + list(grid[1:1 + npts])
+    times = [0.0] + list(grid[1:1 + npts]) + ([float(grid[-1])] if last and npts < 19 else [])
     mb, mc = rb.syk.majoranas(N)
     out = {"workload": f"sparse SYK N={N} (2^{L}), k={cfg['k']}, 1 realisation x 1 state, "
                        f"t in {[float(round(t, 4)) for t in times]} of the 20-point grid on [0, 15], "
@@ -172,15 +177,23 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
         else:
             psi0 = torch.empty(1 << L, dtype=torch.complex64, device="cuda")
             rb.copy(psi0, psi64)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        vals, applies = rb.otoc(ham, w, v, psi0, times, krydim, tol)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
+        vals, per_s, per_ap = [], [], []
+        for t in times:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            val, ap = rb.otoc(ham, w, v, psi0, [t], krydim, tol)
+            torch.cuda.synchronize()
+            per_s.append(time.perf_counter() - t0)
+            per_ap.append(int(ap))
+            vals.append(val[0])
+        vals = np.array(vals)
+        el = float(sum(per_s))
         res[name] = vals
         npt = len(times) - 1   # t = 0 costs no evolve
         out[name] = {"seconds": round(el, 3), "pts_per_s": round(npt / el, 5),
-                     "applies": int(applies), "tol": tol,
+                     "applies": int(sum(per_ap)), "tol": tol,
+                     "seconds_per_point": [round(x, 3) for x in per_s],
+                     "applies_per_point": per_ap,
                      "F": [[round(z.real, 10), round(z.imag, 10)] for z in vals]}
         del ham, w, v
         if dt == "c64":
@@ -188,10 +201,15 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16):
         rb._lib.call("rp_workspace_release")
         torch.cuda.empty_cache()
     f0 = abs(res["fp64_plain"][0])
-    err = float(np.max(np.abs(res["mixed_fp32"] - res["fp64_plain"])) / f0)
-    out["mixed_max_rel_err_vs_fp64"] = err
+    per = np.abs(res["mixed_fp32"] - res["fp64_plain"]) / f0
+    out["mixed_max_rel_err_vs_fp64"] = float(np.max(per))
+    out["mixed_rel_err_per_point"] = [float(x) for x in per]
     out["speedup_mixed_vs_fp64"] = round(out["fp64_plain"]["seconds"] /
                                          out["mixed_fp32"]["seconds"], 3)
+    out["speedup_mixed_vs_fp64_per_point"] = [
+        round(a / b, 3) if b > 0 else None
+        for a, b in zip(out["fp64_plain"]["seconds_per_point"],
+                        out["mixed_fp32"]["seconds_per_point"])]
     return out
 
 
@@ -517,12 +535,13 @@ def cpu_reference(cfg, bits, coeff, alg_bytes, rows, reps):
     env = dict(os.environ)
     env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     env.setdefault("OMP_PROC_BIND", "close")
-    r = subprocess.run([O.REF_DRIVER, "bench_rows", tf, fp, "0", str(rows), str(reps)],
+    drv, isa = O.bench_driver()
+    r = subprocess.run([drv, "bench_rows", tf, fp, "0", str(rows), str(reps)],
                        capture_output=True, text=True, check=True, env=env)
     d = json.loads(r.stdout)
     D = 1 << L
     return {"value": alg_bytes * (rows / D) / d["seconds"] / 1e9, "seconds": d["seconds"],
-            "threads": d["threads"], "rows": rows}
+            "threads": d["threads"], "rows": rows, "isa": isa}
 
 
 def dist_setup(n):
@@ -596,11 +615,10 @@ def run_ours(args):
         tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_max = float(tt.item())
-    value = alg * world / t_max / 1e9
-    achieved = alg / t_step / 1e9
     # the kernel's compulsory DRAM bytes: every distinct source block of the
     # tile window read once per window, plus the write
     alg_dram = info["alg_bytes_dram"]
+    value = alg_dram * world / t_max / 1e9
     achieved_dram = alg_dram / t_step / 1e9
 
     # end to end through the public API with host buffers: every step copies
@@ -631,7 +649,7 @@ def run_ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_e2e = float(tt.item())
     rb._lib.call("rp_workspace_release")
-    e2e_value = alg * world / t_e2e / 1e9
+    e2e_value = alg_dram * world / t_e2e / 1e9
 
     peak, peak_kind = measured_peak()
     traffic = profile_traffic(args.config)
@@ -651,13 +669,22 @@ def run_ours(args):
                 "couplings N(0,1) x the reference's SYK scale; i.i.d. complex Gaussian state",
         "config": {"workload": cfg["workload"], "tile_exp": info["tile_exp"],
                    "source_tile_groups": info["ngroups"], "terms": info["nterms"],
-                   "alg_bytes_per_apply": alg, "parallelism": f"replicas x{world}",
+                   "hbm_bytes_per_apply": alg_dram,
+                   "hbm_bytes_rule": "(G_w + 1) * 2^L * element size: distinct source "
+                                     "blocks of the kernel's tile window, plus the write",
+                   "staged_tile_bytes_per_apply": alg,
+                   "staged_rate_GBps": round(alg / t_step / 1e9, 1),
+                   "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (state >> 126 MB), no flush"},
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes, "ms_per_step": round(t_e2e * 1e3, 3)},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved_dram, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved_dram / peak, 4), "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                       "one launch, from the committed profile summary of this "
+                                       "kernel and workload (not measured in this run)"
+                     if traffic else None,
                      "alg_bytes_per_launch": alg_dram,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
@@ -687,12 +714,15 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
-            cb = cpu_reference(cfg, bits, coeff, alg, rows, 1)
+            cb = cpu_reference(cfg, bits, coeff, alg_dram, rows, 1)
             line["cpu_baseline"] = {"value": round(cb["value"], 4), "unit": "GB/s",
                                     "cores": cb["threads"], "kind": "reference",
                                     "sample": f"reference SpinOp::apply over {rows} of 2^{L} "
                                               f"output rows, same terms, OpenMP "
-                                              f"{cb['threads']} threads, {cb['seconds']:.2f} s"}
+                                              f"{cb['threads']} threads ({cb['isa']} build), "
+                                              f"{cb['seconds']:.2f} s; value = the whole "
+                                              f"apply's HBM bytes x the row fraction / time "
+                                              f"(extrapolated from the sample)"}
         except Exception as e:   # the baseline is reported, never the target
             line["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": os.cpu_count(),
                                     "kind": "reference", "sample": f"failed: {e}"}
@@ -715,8 +745,8 @@ def run_reference(args):
         return
     L = cfg["N"] // 2
     bits, coeff = make_terms(cfg, seed=1000)
-    # the algorithmic bytes are those of our arm's plan (host-side grouping),
-    # so both arms report the same unit for the same work
+    # the bytes are those of our arm's plan (host-side grouping), so both arms
+    # report the same unit for the same work
     alg = alg_bytes_host(L, bits, cfg["dtype"])
     rows = 1 << 19 if cfg["N"] >= 56 else 1 << 17
     times = []
@@ -726,29 +756,39 @@ def run_reference(args):
             times.append(cb["seconds"])
     t = float(np.mean(times))
     value = alg * (rows / (1 << L)) / t / 1e9
+    sample = (f"reference SpinOp::apply (CPUImpl::apply_ops loop) over {rows} of 2^{L} output "
+              f"rows per step, OpenMP {cb['threads']} threads ({cb['isa']} build); value = the "
+              f"whole apply's HBM bytes x the row fraction / time, i.e. extrapolated from the "
+              f"row sample")
     line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "impl": "reference",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (complex64)" if cfg["dtype"] == "c64" else "f64 (complex128)",
             "data": "synthetic (same generator and seed as our arm)",
-            "config": {"workload": cfg["workload"],
-                       "sample": f"{rows} of 2^{L} output rows per step"},
+            "config": {"workload": cfg["workload"], "sample": sample,
+                       "value_is": "extrapolated from a row sample"},
             "cpu_baseline": {"value": round(value, 4), "unit": "GB/s",
-                             "cores": cb["threads"], "kind": "reference",
-                             "sample": f"{rows} of 2^{L} output rows per step"},
+                             "cores": cb["threads"], "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def alg_bytes_host(L, bits, dtype, tile_exp=12):
-    """(G + 1) * 2^L * element size for the default plan (G = distinct x >> B)."""
+def alg_bytes_host(L, bits, dtype, sms=148):
+    """The row kernel's compulsory DRAM bytes, (G_w + 1) * 2^L * element size,
+    computed on the host as the kernel's plan does: tiles of 2^B elements
+    (B = 12 for complex64, 11 for complex128), a window of min(tiles, 2 x SMs)
+    CTAs, G_w = distinct x >> (B + floor(log2 window))."""
     import reapers_b200.syk as S
-    B = min(tile_exp, max(5, L - 8))
+    B = 12 if dtype == "c64" else 11
+    win = min(1 << (L - B), 2 * sms)
+    lw = 0
+    while (2 << lw) <= win:
+        lw += 1
     x = S.xmask(bits)
-    G = len(np.unique(x >> np.uint64(B)))
-    return (G + 1) * (1 << L) * (8 if dtype == "c64" else 16)
+    G_w = len(np.unique(x >> np.uint64(B + lw)))
+    return (G_w + 1) * (1 << L) * (8 if dtype == "c64" else 16)
 
 
 def main():

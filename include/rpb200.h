@@ -76,15 +76,22 @@ typedef struct {
 
 /* --- context ------------------------------------------------------------ */
 /* Select the device and create the stream.  Replaces the static-init
- * GPUContext (inc/gpuimpl.h:496-559); called lazily by every entry point. */
+ * GPUContext (inc/gpuimpl.h:496-559); called lazily by every entry point.
+ * A process stays bound to its first device: rp_init with another device
+ * returns RP_E_INVALID, also after rp_shutdown. */
 int rp_init(int device);
-/* Release cached workspaces and the stream. */
+/* Release cached workspaces, scratch buffers and the stream (a later call
+ * allocates them afresh on the same device). */
 int rp_shutdown(void);
 const char *rp_last_error(void);
 /* GPUImpl::get_device_count (inc/gpuimpl.h:590-592). */
 int rp_device_count(int *count);
 /* The cudaStream_t all calls are ordered on. */
 void *rp_stream(void);
+/* Wait for the stream.  Like GPUImpl::sync_device's error peek
+ * (inc/gpuimpl.h:634-638): returns RP_E_DEVICE if a pipeline wait of an
+ * asynchronous rp_apply / rp_apply_shard gave up since the last check
+ * (that product's output is incomplete), and clears the report. */
 int rp_synchronize(void);
 
 /* --- memory (DeviceVec, inc/gpuimpl.h:405-494) -------------------------- */
@@ -109,12 +116,14 @@ int rp_vec_scale(int dtype, uint64_t n, void *v, double ar, double ai);
 /* GPUImpl::vec_prod: out[0] + i out[1] = <a|b> (conjugate-linear in a),
  * FP64 compensated accumulation */
 int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out);
-/* Same result as rp_vec_dot, but allocates no device memory: for callers
- * that cannot let a library call cudaMalloc (a framework that owns all
- * device memory through its own allocator, or a loop in which cudaMalloc /
- * cudaFree would implicitly synchronise the device).  No counterpart in the
- * reference.  Its scratch is a fixed 16 KB device array (1024 partial sums),
- * so n may be at most 2^28 (larger n returns RP_E_INVALID with a message).
+/* The same inner product as rp_vec_dot to FP64 rounding (the reduction
+ * order differs, so the bits may too), but allocates no device memory: for
+ * callers that cannot let a library call cudaMalloc (a framework that owns
+ * all device memory through its own allocator, or a loop in which
+ * cudaMalloc / cudaFree would implicitly synchronise the device).  No
+ * counterpart in the reference.  Its scratch is a fixed 16 KB device array
+ * (up to 1024 per-block partial sums); n may be at most 2^28 (larger n
+ * returns RP_E_INVALID with a message).
  * The first call on each device looks up the array's device address; make
  * that first call before any stream capture.  All calls share the array:
  * calls that overlap on the GPU race.  Runs on the legacy default stream. */
@@ -144,6 +153,15 @@ int rp_ham_info(rp_ham_t h, rp_ham_info_t *info);
 /* GPUImpl::apply_ops (src/krnl.cu:220-257): out = H in, or out += H in when
  * accumulate != 0.  in and out must differ. */
 int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate);
+/* Test hook of the failure path, no counterpart in the reference: the next
+ * row-kernel launch (states of at least 2^19 complex64 / 2^18 complex128
+ * elements) withholds the tile copy of producer iteration `iteration` in its
+ * first CTA and gives every pipeline wait `wait_polls` polls (1024 to
+ * 2^26).  That CTA's consumers wait on a barrier that nothing completes,
+ * give up, let the copies in flight land and return; the other CTAs finish.
+ * The next rp_synchronize returns RP_E_DEVICE and the context stays usable.
+ * Applies to one launch. */
+int rp_test_withhold_tile(int64_t iteration, uint32_t wait_polls);
 /* out_host[i] = H in_host[i] for i < n: n states in HOST memory (2^len
  * elements of the Hamiltonian's precision each; pinned memory lets the
  * copies run asynchronously).  Pipelined over two device buffer pairs kept by

@@ -207,10 +207,33 @@ def otoc(length, bits, coeff, w, v, psi0, times, krydim=5, tol=np.finfo(float).e
 # The reference itself (prebuilt oracle/_ref/ref_driver)
 # ---------------------------------------------------------------------------
 REF_DRIVER = os.path.join(_HERE, "_ref", "ref_driver")
+# the same driver for x86-64-v4 (AVX-512) hosts: the timed CPU baseline there
+REF_DRIVER_V4 = os.path.join(_HERE, "_ref", "ref_driver_v4")
+_V4_FLAGS = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
 
 
 def ref_available():
     return os.path.exists(REF_DRIVER)
+
+
+def host_is_v4():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = set(line.split(":", 1)[1].split())
+                    return all(x in fl for x in _V4_FLAGS)
+    except OSError:
+        pass
+    return False
+
+
+def bench_driver():
+    """The reference driver built for this host's ISA level (x86-64-v4 where
+    the CPU has AVX-512, else the portable x86-64-v3 build) and its name."""
+    if host_is_v4() and os.path.exists(REF_DRIVER_V4):
+        return REF_DRIVER_V4, "x86-64-v4"
+    return REF_DRIVER, "x86-64-v3"
 
 
 def write_terms(path, length, bits, coeff):

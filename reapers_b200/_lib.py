@@ -77,6 +77,7 @@ _SIGS = {
     "rp_ham_destroy": (C.c_int, [_VP]),
     "rp_ham_info": (C.c_int, [_VP, C.POINTER(HamInfo)]),
     "rp_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "rp_test_withhold_tile": (C.c_int, [C.c_int64, C.c_uint32]),
     "rp_apply_host": (C.c_int, [_VP, C.c_int, C.POINTER(_VP), C.POINTER(_VP)]),
     "rp_apply_shard": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(_VP), _VP, C.c_int]),
     "rp_ipc_export": (C.c_int, [_VP, C.POINTER(IpcHandle)]),

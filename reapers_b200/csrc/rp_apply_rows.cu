@@ -222,6 +222,11 @@ struct RowArgs {
     int ndot;
     double *partials;
     unsigned *err;
+    // polls before a pipeline wait gives up (WAIT_LIMIT), and the failure-path
+    // test hook: CTA 0's producer withholds the tile copy of iteration hold_it
+    // (-1: none), so that its consumers wait on a barrier that never completes
+    uint32_t wait_polls;
+    long hold_it;
 };
 
 constexpr int ROW_P = 256;          // consumer threads = rows per tile
@@ -339,13 +344,14 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
             for (; it < total; ++it) {
                 const int s = (int)(it % S);
                 const unsigned round = (unsigned)(it / S);
-                if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, a.err)) {
+                if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, a.err, a.wait_polls)) {
                     atomicExch(&s_abort, 1);
                     break;
                 }
                 const long ti = it / a.ngroups;
                 const int g = (int)(it - ti * a.ngroups);
                 const uint32_t o = a.tile0 + blockIdx.x + (uint32_t)ti * gridDim.x;
+                if (it == a.hold_it && blockIdx.x == 0) continue;   // test hook: never arrives
                 mbar_arrive_expect_tx(&full[s], ROW_TILE_BYTES);
                 if constexpr (SHARD) {
                     const uint32_t src = (a.gtile0 + o) ^ sgroups[g].xh;
@@ -375,7 +381,7 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
                 const unsigned round = (unsigned)(it / S);
                 const RowGroup gd = sgroups[g];
                 const uint32_t src_hi = (og ^ gd.xh) << B;
-                if (!mbar_wait_bounded(&full[s], round & 1u, a.err)) {
+                if (!mbar_wait_bounded(&full[s], round & 1u, a.err, a.wait_polls)) {
                     ok = false;
                     break;
                 }
@@ -518,10 +524,12 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
     }
     __syncthreads();
     if (s_abort) {
+        // let the copies still in flight land before the CTA exits (the
+        // withheld test copy was never issued)
         if (tid == 0) {
             const long issued = s_issued;
             for (long it = issued - S; it < issued; ++it) {
-                if (it < 0) continue;
+                if (it < 0 || (it == a.hold_it && blockIdx.x == 0)) continue;
                 mbar_wait_bounded(&full[it % S], (unsigned)((it / S) & 1), a.err);
             }
         }
@@ -603,6 +611,23 @@ CUtensorMap make_row_map(const void *base, int len, int dtype) {
     return m;
 }
 
+// The failure-path test hook (rows_test_withhold): armed for one launch.
+struct HoldTest {
+    bool armed = false;
+    long iteration = -1;
+    uint32_t polls = WAIT_LIMIT;
+};
+static HoldTest g_hold;
+
+void rows_test_withhold(long iteration, uint32_t polls) {
+    RP_REQUIRE(iteration >= 0, -2, "the withheld iteration must be non-negative");
+    RP_REQUIRE(polls >= 1024 && polls <= WAIT_LIMIT, -2,
+               "wait_polls must be in [1024, " + std::to_string(WAIT_LIMIT) + "]");
+    g_hold.armed = true;
+    g_hold.iteration = iteration;
+    g_hold.polls = polls;
+}
+
 template <typename Real>
 static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch &l,
                           cudaStream_t st) {
@@ -661,6 +686,13 @@ static void launch_rows_t(const RowPlan &rp, int len, int dtype, const RowLaunch
     a.ndot = l.ndot;
     a.partials = l.partials;
     a.err = l.err;
+    a.wait_polls = WAIT_LIMIT;
+    a.hold_it = -1;
+    if (g_hold.armed) {
+        a.wait_polls = g_hold.polls;
+        a.hold_it = g_hold.iteration;
+        g_hold = HoldTest{};
+    }
     if (shard) {
         RowShardMaps maps;
         std::memset(&maps, 0, sizeof(maps));

@@ -105,6 +105,12 @@ constexpr int ROW_MAX_SHARDS = 8;
 
 void rows_launch(const RowPlan &rp, int len, int dtype, const RowLaunch &l, cudaStream_t st);
 
+// Failure-path test hook: the next row-kernel launch withholds the tile copy
+// of producer iteration `iteration` in CTA 0 and gives every pipeline wait
+// `polls` polls, so that CTA's waits give up and it winds down (error word
+// DEV_ERR_WAIT_TIMEOUT) while the other CTAs finish.  One launch only.
+void rows_test_withhold(long iteration, uint32_t polls);
+
 // 2-D TMA map of a state of 2^len elements at base (rows of 128 bytes, one
 // 256-row tile per box, 128-byte swizzle).
 CUtensorMap make_row_map(const void *base, int len, int dtype);

@@ -35,7 +35,13 @@ static int g_device = -1;
 static KryWorkspace g_ws;
 static ArnoldiResult g_arn;   // the basis of the last rp_arnoldi
 static std::mutex g_mu;
+// Error word of the asynchronous H.psi launches (rp_apply, rp_apply_shard,
+// rp_apply_host): a pipeline wait that gave up sets a bit in it; the next
+// synchronising call reads and clears it (RP_E_DEVICE).
+static unsigned *g_dev_err = nullptr;
 
+// g_err is per thread: entry points failing at once on several host threads
+// each keep their own message.
 void set_error(int code, const std::string &msg) {
     (void)code;
     g_err = msg;
@@ -52,6 +58,22 @@ static void ensure_init() {
     // in both directions, so buffers written by a caller on the default stream
     // (and reads of our results there) need no extra synchronisation.
     RP_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamDefault));
+    if (!g_dev_err) {
+        RP_CUDA(cudaMalloc((void **)&g_dev_err, sizeof(unsigned)));
+        RP_CUDA(cudaMemset(g_dev_err, 0, sizeof(unsigned)));
+    }
+}
+
+// After a stream synchronisation: report (and clear) a wait that gave up in
+// an asynchronous H.psi launch since the last check.
+static void check_device_error() {
+    unsigned herr = 0;
+    RP_CUDA(cudaMemcpy(&herr, g_dev_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (herr) {
+        RP_CUDA(cudaMemset(g_dev_err, 0, sizeof(unsigned)));
+        throw Error{RP_E_DEVICE, "a device-side wait gave up in an H.psi launch (error word " +
+                                     std::to_string(herr) + "); its output is incomplete"};
+    }
 }
 
 static size_t esize(int dtype) { return dtype == RP_C128 ? 16 : 8; }
@@ -94,8 +116,13 @@ extern "C" {
 int rp_init(int device) {
     try {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (g_stream && device != g_device) {
-            throw Error{RP_E_INVALID, "rp_init: the library is already bound to another device"};
+        // The kernels' shared-memory attributes and the SM count are set up
+        // once for the first device; rp_shutdown frees the buffers, streams
+        // and scratch, but the process stays bound to that device.
+        if (g_device >= 0 && device != g_device) {
+            throw Error{RP_E_INVALID, "rp_init: this process is bound to device " +
+                                          std::to_string(g_device) +
+                                          "; another device needs another process"};
         }
         g_device = device;
         ensure_init();
@@ -111,8 +138,12 @@ static void pipe_release();
 int rp_shutdown(void) {
     try {
         std::lock_guard<std::mutex> lk(g_mu);
+        if (g_stream) cudaStreamSynchronize(g_stream);
         workspace_release(g_ws);
         pipe_release();
+        scratch_release_all();
+        if (g_dev_err) cudaFree(g_dev_err);
+        g_dev_err = nullptr;
         if (g_stream) cudaStreamDestroy(g_stream);
         g_stream = nullptr;
         return RP_OK;
@@ -142,7 +173,10 @@ void *rp_stream(void) {
 }
 
 int rp_synchronize(void) {
-    return guarded([&] { RP_CUDA(cudaStreamSynchronize(g_stream)); });
+    return guarded([&] {
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+        check_device_error();
+    });
 }
 
 int rp_alloc(void **ptr, size_t bytes) {
@@ -230,13 +264,11 @@ int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out)
         check_vec(a);
         check_vec(b);
         RP_REQUIRE(out, RP_E_INVALID, "null output pointer");
-        static double *part = nullptr;
-        static double *red = nullptr;
         const int g = reduce_grid();
-        if (!part) {
-            RP_CUDA(cudaMalloc((void **)&part, (size_t)g * 2 * sizeof(double)));
-            RP_CUDA(cudaMalloc((void **)&red, 2 * sizeof(double)));
-        }
+        // partials[g][2], then the reduced pair
+        double *part = static_cast<double *>(
+            scratch_get(SCR_DOT, ((size_t)g + 1) * 2 * sizeof(double), g_stream));
+        double *red = part + (size_t)g * 2;
         VecTable tab{};
         tab.p[0] = a;
         multi_dot_partials(dtype, n, tab, 1, b, part, nullptr, nullptr, g_stream);
@@ -353,8 +385,13 @@ int rp_apply(rp_ham_t h, void *out, const void *in, int accumulate) {
         L.in = in;
         L.out = out;
         L.accumulate = accumulate;
+        L.err = g_dev_err;
         apply_launch(h->plan, L, g_stream);
     });
+}
+
+int rp_test_withhold_tile(int64_t iteration, uint32_t wait_polls) {
+    return guarded([&] { rows_test_withhold((long)iteration, wait_polls); });
 }
 
 int rp_apply_shard(rp_ham_t h, int shard_bits, int shard_rank, const void *const *shards, void *out,
@@ -368,6 +405,7 @@ int rp_apply_shard(rp_ham_t h, int shard_bits, int shard_rank, const void *const
         L.shards = shards;
         L.shard_bits = shard_bits;
         L.shard_rank = shard_rank;
+        L.err = g_dev_err;
         apply_launch(h->plan, L, g_stream);
     });
 }
@@ -536,6 +574,7 @@ int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *ou
                 ApplyLaunch L;
                 L.in = p.din[b];
                 L.out = p.dout[b];
+                L.err = g_dev_err;
                 size_t off = 0, len = bytes;
                 if (nch > 1) {
                     L.tile0 = (uint32_t)c * per;
@@ -555,6 +594,7 @@ int rp_apply_host(rp_ham_t h, int n, const void *const *in_host, void *const *ou
         }
         RP_CUDA(cudaStreamSynchronize(p.s_out));
         RP_CUDA(cudaStreamSynchronize(g_stream));
+        check_device_error();
     });
 }
 

@@ -89,13 +89,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
 }
 
 // Bounded wait on an mbarrier phase.  Returns false (and records the timeout
-// in *err) if the phase did not complete within WAIT_LIMIT polls.
+// in *err, when given) if the phase did not complete within `limit` polls.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity,
-                                                  unsigned *err) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+                                                  unsigned *err, uint32_t limit = WAIT_LIMIT) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
     }
-    atomicOr(err, DEV_ERR_WAIT_TIMEOUT);
+    if (err) atomicOr(err, DEV_ERR_WAIT_TIMEOUT);
     return false;
 }
 

@@ -256,13 +256,9 @@ __global__ void __launch_bounds__(512) k_kry_expm(KryDev *s, cd *hfull, int hcap
 }
 
 double vec_norm_sync(int dtype, uint64_t n, const void *v, KryWorkspace *ws, cudaStream_t st) {
-    static double *scratch = nullptr;
     const int g = reduce_grid();
     double *part = ws && ws->partials ? ws->partials : nullptr;
-    if (!part) {
-        if (!scratch) RP_CUDA(cudaMalloc((void **)&scratch, (size_t)g * 2 * sizeof(double)));
-        part = scratch;
-    }
+    if (!part) part = static_cast<double *>(scratch_get(SCR_NORM, (size_t)g * 2 * sizeof(double), st));
     VecTable tab{};
     tab.p[0] = v;
     multi_dot_partials(dtype, n, tab, 1, v, part, nullptr, nullptr, st);
@@ -488,16 +484,7 @@ void expm_candidates(int m, const double *H, int ncand, const double *fr, const 
     const size_t sb = (size_t)ncand * 10 * m * m * sizeof(cd);
     const size_t need = hb + sb + 2 * ncand * sizeof(double) + (size_t)ncand * m * sizeof(cd);
     // one buffer kept between calls (a step controller calls this every step)
-    static char *buf = nullptr;
-    static size_t cap = 0;
-    if (need > cap) {
-        RP_CUDA(cudaStreamSynchronize(st));
-        if (buf) cudaFree(buf);
-        buf = nullptr;
-        cap = 0;
-        RP_CUDA(cudaMalloc((void **)&buf, need));
-        cap = need;
-    }
+    char *buf = static_cast<char *>(scratch_get(SCR_EXPM, need, st));
     cd *dH = (cd *)buf;
     cd *scr = (cd *)(buf + hb);
     double *dfr = (double *)(buf + hb + sb), *dfi = dfr + ncand;

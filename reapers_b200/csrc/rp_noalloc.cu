@@ -9,13 +9,15 @@
 //
 // Scratch: NOALLOC_MAX_BLOCKS per-block partial pairs (re, im) plus the
 // reduced result, 16 KB + 16 B, resident on every device that loads the
-// library until the process exits.  Each block reduces NOALLOC_BLOCK_ELEMS
-// elements, so vectors longer than NOALLOC_MAX_BLOCKS * NOALLOC_BLOCK_ELEMS
-// (2^28 elements: a 28-qubit state) are rejected.
+// library until the process exits.  The grid is a few blocks per SM (at most
+// NOALLOC_MAX_BLOCKS), each block reducing one contiguous span of a multiple
+// of 256 elements; vectors longer than NOALLOC_MAX_ELEMS (2^28 elements: a
+// 28-qubit state) are rejected.
 //
 // All calls share the one array and it keeps the previous call's contents;
 // every slot a call reads is written by that same call first.  Calls that
 // overlap on the GPU (other streams or host threads) race on the array.
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -25,18 +27,20 @@
 namespace rp {
 
 constexpr int NOALLOC_MAX_BLOCKS = 1024;
-constexpr uint64_t NOALLOC_BLOCK_ELEMS = 1ull << 18;
+constexpr uint64_t NOALLOC_MAX_ELEMS = 1ull << 28;
 constexpr int NOALLOC_THREADS = 256;
+constexpr int NOALLOC_BLOCKS_PER_SM = 4;
 
 // partials[2 * b + {0, 1}] for block b, result at [2 * NOALLOC_MAX_BLOCKS + {0, 1}]
 static __device__ __align__(256) double g_noalloc_scratch[2 * NOALLOC_MAX_BLOCKS + 2];
 
 template <typename Real>
 __global__ void __launch_bounds__(NOALLOC_THREADS)
-    k_dot_blocks(uint64_t n, const Cplx<Real> *a, const Cplx<Real> *b, double *scratch) {
+    k_dot_blocks(uint64_t n, uint64_t span, const Cplx<Real> *a, const Cplx<Real> *b,
+                 double *scratch) {
     __shared__ double s_re[NOALLOC_THREADS / 32], s_im[NOALLOC_THREADS / 32];
-    const uint64_t lo = (uint64_t)blockIdx.x * NOALLOC_BLOCK_ELEMS;
-    const uint64_t hi = lo + NOALLOC_BLOCK_ELEMS < n ? lo + NOALLOC_BLOCK_ELEMS : n;
+    const uint64_t lo = (uint64_t)blockIdx.x * span;
+    const uint64_t hi = lo + span < n ? lo + span : n;
     double sr = 0.0, si = 0.0;
     for (uint64_t k = lo + threadIdx.x; k < hi; k += NOALLOC_THREADS) {
         const Cplx<Real> x = a[k], y = b[k];
@@ -86,40 +90,51 @@ extern "C" int rp_vec_dot_noalloc(int dtype, uint64_t n, const void *a, const vo
     // only names a host-side stand-in, never a device address.
     static std::mutex mu;
     static double *addr[64] = {nullptr};
+    static int sms[64] = {0};
     try {
         RP_REQUIRE(dtype == RP_C64 || dtype == RP_C128, RP_E_INVALID,
                    "dtype must be RP_C64 (1) or RP_C128 (2)");
         RP_REQUIRE(a && b && out, RP_E_INVALID, "null pointer");
-        RP_REQUIRE(n <= (uint64_t)NOALLOC_MAX_BLOCKS * NOALLOC_BLOCK_ELEMS, RP_E_INVALID,
+        RP_REQUIRE(n <= NOALLOC_MAX_ELEMS, RP_E_INVALID,
                    "rp_vec_dot_noalloc: vector length " + std::to_string(n) +
-                       " exceeds the fixed scratch limit of " +
-                       std::to_string((uint64_t)NOALLOC_MAX_BLOCKS * NOALLOC_BLOCK_ELEMS) +
+                       " exceeds the fixed scratch limit of " + std::to_string(NOALLOC_MAX_ELEMS) +
                        " elements");
         int dev = 0;
         RP_CUDA(cudaGetDevice(&dev));
         RP_REQUIRE(dev >= 0 && dev < 64, RP_E_INVALID, "device ordinal out of range");
         double *scratch;
+        int nsm;
         {
             std::lock_guard<std::mutex> lk(mu);
             if (!addr[dev]) {
                 void *p = nullptr;
                 RP_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                RP_CUDA(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
                 addr[dev] = static_cast<double *>(p);
             }
             scratch = addr[dev];
+            nsm = sms[dev];
         }
         if (n == 0) {
             out[0] = out[1] = 0.0;
             return RP_OK;
         }
-        const int nblocks = (int)((n + NOALLOC_BLOCK_ELEMS - 1) / NOALLOC_BLOCK_ELEMS);
+        // a few blocks per SM, each over a span of whole 256-element steps
+        uint64_t want = (n + NOALLOC_THREADS - 1) / NOALLOC_THREADS;
+        want = std::min<uint64_t>(want, (uint64_t)NOALLOC_BLOCKS_PER_SM * std::max(1, nsm));
+        want = std::min<uint64_t>(want, NOALLOC_MAX_BLOCKS);
+        uint64_t span = (n + want - 1) / want;
+        span = (span + NOALLOC_THREADS - 1) / NOALLOC_THREADS * NOALLOC_THREADS;
+        const int nblocks = (int)((n + span - 1) / span);
         // Ordered on the legacy default stream, like a caller's own work.
         if (dtype == RP_C128)
             k_dot_blocks<double><<<nblocks, NOALLOC_THREADS>>>(
-                n, static_cast<const Cplx<double> *>(a), static_cast<const Cplx<double> *>(b), scratch);
+                n, span, static_cast<const Cplx<double> *>(a), static_cast<const Cplx<double> *>(b),
+                scratch);
         else
             k_dot_blocks<float><<<nblocks, NOALLOC_THREADS>>>(
-                n, static_cast<const Cplx<float> *>(a), static_cast<const Cplx<float> *>(b), scratch);
+                n, span, static_cast<const Cplx<float> *>(a), static_cast<const Cplx<float> *>(b),
+                scratch);
         RP_CUDA(cudaGetLastError());
         k_dot_finish<<<1, 32>>>(nblocks, scratch);
         RP_CUDA(cudaGetLastError());

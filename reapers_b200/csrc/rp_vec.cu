@@ -10,6 +10,31 @@ namespace rp {
 
 int reduce_grid() { return 2 * num_sms(); }
 
+static void *g_scratch[SCR_COUNT] = {};
+static size_t g_scratch_cap[SCR_COUNT] = {};
+
+void *scratch_get(int slot, size_t bytes, cudaStream_t st) {
+    if (bytes > g_scratch_cap[slot]) {
+        if (g_scratch[slot]) {
+            RP_CUDA(cudaStreamSynchronize(st));
+            cudaFree(g_scratch[slot]);
+        }
+        g_scratch[slot] = nullptr;
+        g_scratch_cap[slot] = 0;
+        RP_CUDA(cudaMalloc(&g_scratch[slot], bytes));
+        g_scratch_cap[slot] = bytes;
+    }
+    return g_scratch[slot];
+}
+
+void scratch_release_all() {
+    for (int s = 0; s < SCR_COUNT; s++) {
+        if (g_scratch[s]) cudaFree(g_scratch[s]);
+        g_scratch[s] = nullptr;
+        g_scratch_cap[s] = 0;
+    }
+}
+
 static inline int blocks_for(uint64_t n, int threads, int cap) {
     uint64_t b = (n + threads - 1) / threads;
     return (int)(b < (uint64_t)cap ? (b ? b : 1) : cap);

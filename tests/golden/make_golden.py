@@ -23,6 +23,18 @@ Fixtures (numpy .npz):
                            forms (full terms; H_LL, H_RR), and the parity-block
                            OTOC of examples/syk.cc at t = 0, 0.4, 1.1 with
                            op = LR of b_{N-2} (m = 10, tol 1e-12)
+  dense_syk_N24_t10.npz    the dense SYK N = 24 evolve at all ten points
+                           t = 0.5, 1.0, ..., 5.0 (m = 20, tol = 1e-12)
+  evolve_sparse_N40.npz    sparse SYK N = 40 (20 qubits, k = 8, 320 terms,
+                           seeded project generator), FP64 State::evolve to
+                           t = 10 with m = 30 at the reference's default tol
+                           (FP64 epsilon): its call counts, the final state at
+                           4096 sampled indices plus the first and last, its
+                           norm, and its projections onto 8 seeded random
+                           vectors (a checksum of the whole state)
+
+Usage: make_golden.py [name ...] regenerates only the named fixtures (file
+stems, e.g. dense_syk_N24_t10); without names, all of them.
 """
 import os
 import sys
@@ -37,8 +49,61 @@ from oracle import oracle as O  # noqa: E402
 import reapers_b200.syk as S  # noqa: E402
 
 
+N40_SEED, N40_PSI_SEED, N40_PROBE_SEED = 4040, 4041, 4042
+
+
+def n40_problem():
+    """The 20-qubit evolve problem of evolve_sparse_N40.npz: Hamiltonian,
+    start state and the probe vectors (all regenerated from seeds)."""
+    L = 20
+    bits, coeff = S.sparse_syk(40, k=8, seed=N40_SEED)
+    rng = np.random.default_rng(N40_PSI_SEED)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    prng = np.random.default_rng(N40_PROBE_SEED)
+    probes = prng.standard_normal((8, 1 << L)) + 1j * prng.standard_normal((8, 1 << L))
+    idx = np.unique(np.concatenate([[0, (1 << L) - 1],
+                                    prng.integers(0, 1 << L, size=4096)])).astype(np.int64)
+    return L, bits, coeff, psi, probes, idx
+
+
+def make_dense_t10(R):
+    L, b, c = R.syk(24, 0.0, 1.0, 1)
+    rng = np.random.default_rng(2024)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    times = [0.5 * k for k in range(1, 11)]
+    outs, applies, prods = [], [], []
+    for t in times:
+        o, st = R.evolve(L, b, c, psi, t, 0.0, 20, 1e-12)
+        outs.append(o)
+        applies.append(st["applies"])
+        prods.append(st["prods"])
+    np.savez_compressed(os.path.join(HERE, "dense_syk_N24_t10.npz"), bits=b, coeff=c, len=L,
+                        psi0=psi, times=np.array(times), out=np.array(outs),
+                        applies=np.array(applies), prods=np.array(prods), krydim=20, tol=1e-12)
+
+
+def make_sparse_n40(R):
+    L, bits, coeff, psi, probes, idx = n40_problem()
+    tol = float(np.finfo(np.float64).eps)
+    o, st = R.evolve(L, bits, coeff, psi, 10.0, 0.0, 30, tol)
+    np.savez_compressed(os.path.join(HERE, "evolve_sparse_N40.npz"), bits=bits, coeff=coeff,
+                        len=L, t=10.0, beta=0.0, krydim=30, tol=tol, idx=idx, vals=o[idx],
+                        norm=np.linalg.norm(o), proj=probes.conj() @ o,
+                        applies=st["applies"], prods=st["prods"], ref_seconds=st["seconds"],
+                        seeds=np.array([N40_SEED, N40_PSI_SEED, N40_PROBE_SEED]))
+
+
 def main():
-    R = O.RefDriver(threads=8)
+    R = O.RefDriver(threads=os.cpu_count())
+    only = set(sys.argv[1:])
+    if only:
+        if "dense_syk_N24_t10" in only:
+            make_dense_t10(R)
+        if "evolve_sparse_N40" in only:
+            make_sparse_n40(R)
+        return
     for N in range(4, 22, 2):
         L, b, c = R.majorana(N)
         np.savez_compressed(os.path.join(HERE, f"majorana_N{N}.npz"), bits=b, coeff=c)
@@ -119,6 +184,8 @@ def main():
                         ll_bits=llb, ll_coeff=llc, rr_bits=rrb, rr_coeff=rrc, len=Lb, psi0=psi,
                         times=np.array(times), F=F, op_bits=np.array([ob]),
                         op_coeff=np.array([oc]), krydim=10, tol=1e-12)
+    make_dense_t10(R)
+    make_sparse_n40(R)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -85,3 +85,71 @@ def test_parity_block_otoc_reference_fixture(cuda):
     F, applies = rb.otoc_block(ll, rr, op, psi0, g["times"], int(g["krydim"]), float(g["tol"]))
     assert np.abs(F - g["F"]).max() <= 1e-12 * abs(g["F"][0]), (F, g["F"])
     assert applies > 0
+
+
+def test_dense_syk_n24_evolve_all_ten_points(cuda):
+    """The dense SYK N = 24 workload at all ten time points t = 0.5 .. 5.0
+    (m = 20, tol 1e-12) against the reference's own FP64 State::evolve:
+    final states within 1e-12, H.psi and inner-product counts identical."""
+    g = gold("dense_syk_N24_t10.npz")
+    L = int(g["len"])
+    assert len(g["times"]) == 10
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    for k, t in enumerate(g["times"]):
+        x = dev(g["psi0"])
+        st = rb.evolve(ham, x, float(t), 0.0, int(g["krydim"]), float(g["tol"]))
+        o = x.cpu().numpy()
+        assert np.linalg.norm(o - g["out"][k]) / np.linalg.norm(g["out"][k]) < 1e-12, t
+        assert st["applies"] == g["applies"][k], t
+        assert st["prods"] == g["prods"][k], t
+
+
+def _n40_problem():
+    """Regenerates the evolve_sparse_N40 problem from its seeds (the same code
+    as tests/golden/make_golden.py:n40_problem, restated here so that the
+    GPU tests need no fixture script)."""
+    g = gold("evolve_sparse_N40.npz")
+    L = int(g["len"])
+    s_ham, s_psi, s_probe = (int(v) for v in g["seeds"])
+    bits, coeff = rb.syk.sparse_syk(40, k=8, seed=s_ham)
+    assert np.array_equal(bits, g["bits"]) and np.array_equal(coeff, g["coeff"])
+    rng = np.random.default_rng(s_psi)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    prng = np.random.default_rng(s_probe)
+    probes = prng.standard_normal((8, 1 << L)) + 1j * prng.standard_normal((8, 1 << L))
+    return g, L, psi, probes
+
+
+def test_sparse_syk_n40_evolve_t10_reference_fixture(cuda):
+    """Evolve parity at size: 20 qubits (sparse SYK N = 40, k = 8, 320 terms),
+    t = 10, m = 30, tol = FP64 epsilon, the reference's own FP64
+    State::evolve as the oracle.  The FP64 GPU evolve matches it within 1e-12
+    on 4096 sampled entries and on 8 projections of the whole state (a
+    checksum), with identical H.psi and inner-product counts; the mixed path
+    (FP32 vectors and H.psi, FP64 Krylov internals, tol = FP32 epsilon) is
+    within 1e-5 of it (its error is printed)."""
+    g, L, psi, probes = _n40_problem()
+    ham = rb.Hamiltonian(L, g["bits"], g["coeff"], "c128")
+    x = dev(psi)
+    st = rb.evolve(ham, x, float(g["t"]), 0.0, int(g["krydim"]), float(g["tol"]))
+    o = x.cpu().numpy()
+    idx = g["idx"]
+    assert np.linalg.norm(o[idx] - g["vals"]) / np.linalg.norm(g["vals"]) < 1e-12
+    assert abs(np.linalg.norm(o) - float(g["norm"])) < 1e-12
+    proj = probes.conj() @ o
+    assert np.abs(proj - g["proj"]).max() < 1e-12 * np.abs(g["proj"]).max() * 10
+    assert st["applies"] == int(g["applies"]) and st["prods"] == int(g["prods"])
+    ham.close()
+    # the mixed path on the same problem, against the reference's FP64 result
+    hm = rb.Hamiltonian(L, g["bits"], g["coeff"], "c64")
+    xm = torch.empty(1 << L, dtype=torch.complex64, device=cuda)
+    rb.copy(xm, dev(psi))
+    rb.evolve(hm, xm, float(g["t"]), 0.0, int(g["krydim"]), float(np.finfo(np.float32).eps))
+    om = xm.cpu().numpy().astype(np.complex128)
+    err_rows = np.linalg.norm(om[idx] - g["vals"]) / np.linalg.norm(g["vals"])
+    err_proj = np.abs(probes.conj() @ om - g["proj"]).max() / np.abs(g["proj"]).max()
+    print(f"mixed vs reference FP64 at 20 qubits, t = 10: rows {err_rows:.2e}, "
+          f"projections {err_proj:.2e}")
+    assert err_rows < 1e-5 and err_proj < 1e-5
+    hm.close()

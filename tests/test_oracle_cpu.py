@@ -151,6 +151,24 @@ def test_dense_syk_n24_evolve_matches_reference():
         assert st["prods"] == g["prods"][k]
 
 
+def test_ten_point_fixture_agrees_with_the_oracle_pinned_one():
+    """dense_syk_N24_t10.npz (all ten points of the dense SYK N = 24 workload)
+    and dense_syk_N24.npz, whose points the oracle reproduces above, come from
+    two builds of the reference driver: the same quartets and start state,
+    couplings equal to 1e-12 relative (the two builds round the coupling
+    scale's arithmetic differently), and at the shared times t = 0.5, 2.5,
+    5.0 the same counts and states within 1e-13."""
+    a, b = gold("dense_syk_N24.npz"), gold("dense_syk_N24_t10.npz")
+    assert np.array_equal(a["bits"], b["bits"])
+    assert np.all(np.abs(a["coeff"] - b["coeff"]) <= 1e-12 * np.abs(a["coeff"]))
+    assert np.array_equal(a["psi0"], b["psi0"])
+    assert np.allclose(b["times"], 0.5 * np.arange(1, 11))
+    for k, t in enumerate(a["times"]):
+        j = int(np.argmin(np.abs(b["times"] - t)))
+        assert np.linalg.norm(a["out"][k] - b["out"][j]) < 1e-13
+        assert a["applies"][k] == b["applies"][j] and a["prods"][k] == b["prods"][j]
+
+
 def test_imaginary_time_evolve_matches_reference():
     g = gold("evolve_sparse_N20.npz")
     o, st = O.evolve(int(g["len"]), g["bits"], g["coeff"], g["psi0"], float(g["t"]),
