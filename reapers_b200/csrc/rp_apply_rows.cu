@@ -222,9 +222,10 @@ struct RowArgs {
     int ndot;
     double *partials;
     unsigned *err;
-    // polls before a pipeline wait gives up (WAIT_LIMIT), and the failure-path
-    // test hook: CTA 0's producer withholds the tile copy of iteration hold_it
-    // (-1: none), so that its consumers wait on a barrier that never completes
+    // the failure-path test hook: CTA 0's producer withholds the tile copy of
+    // iteration hold_it (-1: none), so that its consumers wait on a barrier
+    // that never completes, and CTA 0's pipeline waits give up after
+    // wait_polls polls (every other wait: WAIT_LIMIT)
     uint32_t wait_polls;
     long hold_it;
 };
@@ -334,6 +335,7 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
     const int ntile_iters =
         (int)blockIdx.x < a.ntiles ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const long total = (long)ntile_iters * a.ngroups;
+    const uint32_t polls = blockIdx.x == 0 ? a.wait_polls : WAIT_LIMIT;
 
     if (warp == ROW_NW) {
         if (lane == 0) {
@@ -344,7 +346,7 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
             for (; it < total; ++it) {
                 const int s = (int)(it % S);
                 const unsigned round = (unsigned)(it / S);
-                if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, a.err, a.wait_polls)) {
+                if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, a.err, polls)) {
                     atomicExch(&s_abort, 1);
                     break;
                 }
@@ -381,7 +383,7 @@ __device__ __forceinline__ void apply_rows_body(const CUtensorMap *maps, const R
                 const unsigned round = (unsigned)(it / S);
                 const RowGroup gd = sgroups[g];
                 const uint32_t src_hi = (og ^ gd.xh) << B;
-                if (!mbar_wait_bounded(&full[s], round & 1u, a.err, a.wait_polls)) {
+                if (!mbar_wait_bounded(&full[s], round & 1u, a.err, polls)) {
                     ok = false;
                     break;
                 }

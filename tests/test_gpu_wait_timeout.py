@@ -15,7 +15,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-POLLS = 1 << 14   # the test's wait limit (polls); the default is 2^26
+POLLS = 1 << 16   # the first CTA's wait limit in the test (polls); the default is 2^26
 
 
 @pytest.mark.parametrize("dtype,L", [("c64", 20), ("c128", 19)])
