@@ -322,6 +322,99 @@ def shard_leg(ham, x, L, reps=3):
     return out
 
 
+class DeviceClock:
+    """CUDA events on the library stream (every apply of a sharded leg ends
+    on it; the exchanges before it are ordered ahead through the legacy
+    default stream, which the library's blocking stream follows)."""
+
+    def __init__(self):
+        import torch
+        import reapers_b200 as rb
+        self.st = rb.stream()
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        self.e0.record(self.st)
+
+    def stop(self):
+        self.e1.record(self.st)
+        self.e1.synchronize()
+        return self.e0.elapsed_time(self.e1) / 1e3
+
+
+def sharded_dist_leg(comm, L, bits, coeff, dtype, steps, warmup, modes=("stage", "peer"),
+                     full=None, make_state=None, clock=None):
+    """The reference's multi-GPU split (inc/gpuimpl.h:426-432, src/krnl.cu:96-114)
+    across the ranks of a process group: one state of 2^L elements split by its
+    top k qubits over 2^k ranks, one shard per rank, and H.psi through
+    reapers_b200.sharded.ShardedHamiltonian in each exchange mode --
+    "stage" (every partner shard the terms reach swapped whole by NCCL
+    send/recv, then one row-kernel launch) and "peer" (no copy: the launch
+    reads the partner shards in the peers' memory over NVLink through CUDA
+    IPC mappings, plain loads, no multicast).  Every rank holds the whole
+    input (the same seeded state), so it also checks its output shard against
+    the single-GPU apply of the full state (bit-identical expected).  Timing:
+    `steps` applies after `warmup`, barrier and device synchronisation on
+    both sides, device time (clock), the max over ranks.
+
+    full / make_state / clock: the full operator class (the library's
+    Hamiltonian unless given), a function making the full input state, and
+    the timer (CUDA events on the library stream unless given) -- injectable
+    so that a CPU process group (gloo) can drive the same plumbing."""
+    from reapers_b200 import sharded as SH
+    world = comm.world
+    k = world.bit_length() - 1
+    r = comm.owned()[0]
+    n = 1 << (L - k)
+    if full is None:
+        import reapers_b200 as rb
+        full = rb.Hamiltonian
+    xfull = make_state()
+    ref_op = full(L, bits, coeff, dtype)
+    ref = _full_apply(ref_op, xfull)
+    ref_op.close()
+    xs = xfull[r * n:(r + 1) * n].clone()
+    del xfull
+    clock = clock or DeviceClock()
+    out = {"workload": f"one state of 2^{L} elements split by its top {k} qubits over {world} "
+                       f"ranks (one shard of 2^{L - k} per rank), H.psi per exchange mode",
+           "modes": {}}
+    for mode in modes:
+        ham = SH.ShardedHamiltonian(L, bits, coeff, comm, dtype, exchange=mode, full=full)
+        x = SH.Shards(comm, {r: xs})
+        y = SH.Shards.empty_like(x)
+        if mode == "peer":
+            x.share()
+        for _ in range(warmup):
+            ham.apply(y, x)
+        comm.barrier()
+        clock.start()
+        for _ in range(steps):
+            ham.apply(y, x)
+        t = clock.stop()
+        comm.barrier()
+        same = bool((y.t[r] == ref[r * n:(r + 1) * n]).all())
+        times = comm.all_gather_object(t)
+        oks = comm.all_gather_object(same)
+        t_max = max(times)
+        out["modes"][mode] = {"ms_per_apply": round(t_max / steps * 1e3, 4),
+                              "ms_per_apply_by_rank": [round(v / steps * 1e3, 4) for v in times],
+                              "bit_identical_to_full_apply": all(oks),
+                              "partner_offsets": list(getattr(ham, "offsets", []))}
+        if mode == "peer":
+            x.unshare()
+        ham.close()
+        del x, y
+    return out
+
+
+def _full_apply(op, x):
+    y = x.clone()
+    op.apply(y, x)
+    return y
+
+
 def _tfim_chain(L, J=1.0, h=0.7):
     """Transverse-field Ising chain: J Z_i Z_{i+1} (open) + h X_i."""
     bits = [(1 << (2 * i + 1)) | (1 << (2 * i + 3)) for i in range(L - 1)]
@@ -371,19 +464,21 @@ def spin_chain_leg(clocks=None, L=28, reps=10):
     return out
 
 
-def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40),
-              seq_per_size=2, tune=True):
-    """Batched OTOC sample: nreal disorder realisations x nstates random
-    states, sparse SYK k = 8 with N cycling over `sizes` (16/18/20 qubits),
-    t = the first `npts` non-zero points of 40 on [0, 20], m = krydim; one
-    persistent launch per time step in a CUDA graph, tile exponents from the
-    autotuner.  Compared with the same problems run one at a time through the
-    single-problem mixed path (rp_evolve), on seq_per_size problems per size."""
+def batch_leg(seed=0, points=(1, 2, 20, 39), krydim=16, nreal=64, nstates=8,
+              sizes=(32, 36, 40), seq_per_size=2, tune=True):
+    """The batched OTOC workload: nreal disorder realisations x nstates random
+    states (64 x 8 = 512 problems), sparse SYK k = 8 with N cycling over
+    `sizes` (16/18/20 qubits), at the `points` of the 40-point grid on
+    [0, 20] (default: t = 0.51, 1.03, 10.26 and 20), m = krydim; one
+    persistent launch per time step in a CUDA graph, tile loop and team size
+    (or the single-problem path) per size from the autotuner.  Compared with
+    the same problems run one at a time through the single-problem mixed path
+    (rp_evolve), on seq_per_size problems per size."""
     import torch
     import reapers_b200 as rb
     from reapers_b200 import autotune
     grid = np.linspace(0.0, 20.0, 40)
-    times = np.array(list(grid[1:1 + npts]))
+    times = np.array([grid[i] for i in points])
     problems = []
     for r in range(nreal):
         N = sizes[r % len(sizes)]
@@ -395,12 +490,18 @@ def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40)
             problems.append(dict(len=L, bits=bits, coeff=coeff, w=(mb[N - 1:N], mc[N - 1:N]),
                                  v=(mb[N - 2:N - 1], mc[N - 2:N - 1]), psi0=psi, N=N))
     tol = float(np.finfo(np.float32).eps)
+    t0 = time.perf_counter()
     tuned = autotune.tune(problems, krydim=krydim, tol=tol) if tune else {}
+    t_tune = time.perf_counter() - t0
     out = {"workload": f"{nreal} sparse-SYK realisations (k=8, N cycling {list(sizes)}) x "
                        f"{nstates} states = {len(problems)} problems, t in "
                        f"{[float(round(t, 4)) for t in times]} of 40 points on [0, 20], m={krydim}",
+           "paths": {k: v.get("path", "batched") for k, v in tuned.items()},
            "tiles": {k: v["tile"] for k, v in tuned.items()},
-           "teams": {k: v["team"] for k, v in tuned.items()}, "per_size": {}}
+           "teams": {k: v["team"] for k, v in tuned.items()},
+           "tuning_seconds": round(t_tune, 2),
+           "tuning_probe_seconds": {k: v["seconds"] for k, v in tuned.items()},
+           "per_size": {}}
     tot_batch = tot_seq = tot_best = 0.0
     err = 0.0
     for N in sizes:
@@ -430,7 +531,11 @@ def batch_leg(seed=0, npts=2, krydim=16, nreal=64, nstates=2, sizes=(32, 36, 40)
         r_s = min(seq_per_size, len(sub)) * len(times) / el2
         out["per_size"][f"N{N}"] = {"problems": len(sub), "batched_pts_per_s": round(r_b, 3),
                                     "sequential_pts_per_s": round(r_s, 3),
-                                    "batched_applies": int(ap.sum())}
+                                    "batched_seconds": round(el, 3),
+                                    "path": sub[0].get("path", "batched"),
+                                    "batched_applies": int(ap.sum()),
+                                    "applies_per_problem_per_point": [
+                                        round(float(v), 1) for v in ap.mean(axis=0)]}
         tot_batch += pts / r_b
         tot_seq += pts / r_s
         tot_best += pts / max(r_b, r_s)
@@ -553,7 +658,7 @@ def dist_setup(n):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     return world, rank, local
 
@@ -692,6 +797,17 @@ def run_ours(args):
                      "term_applications_per_s": info["nterms"] * (1 << L) / t_step},
         "clocks": clocks,
     }
+    # the reference's multi-GPU split of one state (N > 1): every rank takes
+    # part, so it runs before the single-GPU legs
+    if world > 1 and (world & (world - 1)) == 0 and world <= 8 and not args.no_shard:
+        from reapers_b200 import sharded as SH
+        ham.close()
+        del x, ham
+        torch.cuda.empty_cache()
+        sbits, scoeff = make_terms(cfg, seed=1000)
+        line["sharded_split_syk56"] = sharded_dist_leg(
+            SH.ProcessGroupComm(), L, sbits, scoeff, cfg["dtype"], steps=10, warmup=3,
+            make_state=lambda: rb.random_state(L, cfg["dtype"], seed=7, normalize=False))
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1

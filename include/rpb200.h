@@ -214,6 +214,30 @@ int rp_evolve(rp_ham_t h, void *psi, double t, double beta, int krydim, double t
  * buffers of rp_apply_host. */
 int rp_workspace_release(void);
 
+/* --- exact diagonalisation (the dense GPU path: DevSumOps::get_matrix,
+ * get_eigensystem and _matexp, inc/gpuimpl.h:1180-1263, GPUImpl::mat_mul;
+ * used by ExactDiagonalization, inc/algo.h:29-54) ------------------------- */
+typedef struct rp_dense *rp_dense_t;
+/* The dense matrix of a Hermitian Pauli sum on len <= 15 qubits (same term
+ * arguments as rp_ham_create), built on the device from the term table, and
+ * its eigensystem (library eigensolver, heevd, in the dtype's precision):
+ * eigenvalues ascending, eigenvectors the columns of a dim x dim matrix. */
+int rp_dense_create(rp_dense_t *d, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                    const double *coeff);
+/* evals: 2^len doubles, ascending. */
+int rp_dense_eigenvalues(rp_dense_t d, double *evals);
+/* out (device vector, 2^len elements of the dtype) = eigenvector `index`:
+ * the eigensystem column copy of ExactDiagonalization::ground_state. */
+int rp_dense_eigenvector(rp_dense_t d, int64_t index, void *out);
+/* out (device, 2^len x 2^len, column-major, the dtype) = exp((cr + i ci) H)
+ * = V diag(exp((cr + i ci) lambda)) V^H (DevSumOps::_matexp). */
+int rp_dense_expm(rp_dense_t d, double cr, double ci, void *out);
+int rp_dense_destroy(rp_dense_t d);
+/* res = mat vec for a dense dim x dim column-major device matrix
+ * (GPUImpl::mat_mul, inc/gpuimpl.h:1003-1021): FP64 accumulation, fixed
+ * summation order; res and vec distinct. */
+int rp_mat_vec(int dtype, uint64_t dim, const void *mat, const void *vec, void *res);
+
 /* --- time-stepped Krylov primitives (no reference counterpart: the
  * reference only has the restarted evolve; these let a step controller
  * advance exp(-i dt H) psi one sub-step at a time) ------------------------ */

@@ -299,11 +299,31 @@ class BatchOTOC:
     qubit counts) run by one persistent launch per time step (rp_batch_*).
 
     problems: list of dicts with keys len, bits, coeff, w (bits, coeff),
-    v (bits, coeff), psi0 (complex64 CUDA tensor) and optionally tile (8..11)
-    and team (CTAs per problem: 1, 2, 4, 8 or 16).  FP32 vectors, FP64 Krylov
+    v (bits, coeff), psi0 (complex64 CUDA tensor) and optionally tile (8..12),
+    team (CTAs per problem: 1, 2, 4, 8 or 16) and path ('batched', the
+    default, or 'single': the autotuner found the single-problem path faster
+    for this shape, so the problem runs alone on the whole GPU through
+    ``otoc`` after the batched launches).  FP32 vectors, FP64 Krylov
     internals (the mixed-precision form)."""
 
     def __init__(self, problems, krydim=16, tol=1.2e-7, max_restarts=16):
+        self.n = len(problems)
+        self.krydim, self.tol = int(krydim), float(tol)
+        self._single = [i for i, p in enumerate(problems) if p.get("path") == "single"]
+        self._batched = [i for i, p in enumerate(problems) if p.get("path") != "single"]
+        self._singles = []
+        for i in self._single:
+            p = problems[i]
+            if _tcode(p["psi0"]) != RP_C64:
+                raise ValueError("batched states are complex64")
+            self._singles.append((Hamiltonian(p["len"], p["bits"], p["coeff"], "c64"),
+                                  Hamiltonian(p["len"], *p["w"], "c64"),
+                                  Hamiltonian(p["len"], *p["v"], "c64"), p["psi0"]))
+        self._h = None
+        if self._batched:
+            self._create([problems[i] for i in self._batched], krydim, tol, max_restarts)
+
+    def _create(self, problems, krydim, tol, max_restarts):
         n = len(problems)
         self._keep = problems
         lens = (C.c_int * n)(*[int(p["len"]) for p in problems])
@@ -334,21 +354,36 @@ class BatchOTOC:
         _lib.call("rp_batch_create_ex", C.byref(h), n, lens, nterms, bitp, coefp, wb, wc, vb, vc,
                   psis, tiles, teams, int(krydim), float(tol), int(max_restarts))
         self._h = h
-        self.n = n
+        self._nb = n
 
     def run(self, times, use_graph=True):
-        """Returns (F[n, ntimes] complex, applies[n, ntimes])."""
+        """Returns (F[n, ntimes] complex, applies[n, ntimes]): the batched
+        problems by one persistent launch per time step (and team size),
+        captured in a CUDA graph when use_graph, then the single-path ones."""
         times = np.ascontiguousarray(times, dtype=np.float64)
         k = len(times)
-        F = np.zeros(2 * self.n * k)
-        ap = np.zeros(self.n * k, np.int32)
-        _lib.call("rp_batch_otoc", self._h, k, times.ctypes.data_as(C.POINTER(C.c_double)),
-                  F.ctypes.data_as(C.POINTER(C.c_double)),
-                  ap.ctypes.data_as(C.POINTER(C.c_int)), 1 if use_graph else 0)
-        return F.view(np.complex128).reshape(self.n, k), ap.reshape(self.n, k)
+        Fall = np.zeros((self.n, k), dtype=np.complex128)
+        apall = np.zeros((self.n, k), np.int32)
+        if self._h is not None:
+            F = np.zeros(2 * self._nb * k)
+            ap = np.zeros(self._nb * k, np.int32)
+            _lib.call("rp_batch_otoc", self._h, k, times.ctypes.data_as(C.POINTER(C.c_double)),
+                      F.ctypes.data_as(C.POINTER(C.c_double)),
+                      ap.ctypes.data_as(C.POINTER(C.c_int)), 1 if use_graph else 0)
+            Fall[self._batched] = F.view(np.complex128).reshape(self._nb, k)
+            apall[self._batched] = ap.reshape(self._nb, k)
+        for i, (ham, w, v, psi0) in zip(self._single, self._singles):
+            for j, t in enumerate(times):
+                val, a = otoc(ham, w, v, psi0, [t], self.krydim, self.tol)
+                Fall[i, j] = val[0]
+                apall[i, j] = a
+        return Fall, apall
 
     def probe(self, napplies=2):
-        """Device ms of one launch doing napplies H.psi products per problem."""
+        """Device ms of one launch doing napplies H.psi products per batched
+        problem."""
+        if self._h is None:
+            raise ValueError("no problem of this batch runs on the batched path")
         ms = C.c_double()
         _lib.call("rp_batch_probe", self._h, int(napplies), C.byref(ms))
         return ms.value
@@ -357,6 +392,10 @@ class BatchOTOC:
         if getattr(self, "_h", None):
             _lib.load().rp_batch_destroy(self._h)
             self._h = None
+        for trio in getattr(self, "_singles", []):
+            for h in trio[:3]:
+                h.close()
+        self._singles = []
 
     def __del__(self):
         try:

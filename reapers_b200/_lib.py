@@ -91,6 +91,13 @@ _SIGS = {
     "rp_expm_first_column": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_int,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]),
+    "rp_dense_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, C.c_uint64,
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
+    "rp_dense_eigenvalues": (C.c_int, [_VP, C.POINTER(C.c_double)]),
+    "rp_dense_eigenvector": (C.c_int, [_VP, C.c_int64, _VP]),
+    "rp_dense_expm": (C.c_int, [_VP, C.c_double, C.c_double, _VP]),
+    "rp_dense_destroy": (C.c_int, [_VP]),
+    "rp_mat_vec": (C.c_int, [C.c_int, C.c_uint64, _VP, _VP, _VP]),
     "rp_mlp_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, C.c_uint64]),
     "rp_mlp_num_params": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "rp_mlp_get_params": (C.c_int, [_VP, C.POINTER(C.c_float)]),

@@ -11,6 +11,7 @@
 #include "../../include/rpb200.h"
 #include "rp_apply.cuh"
 #include "rp_batch.cuh"
+#include "rp_dense.cuh"
 #include "rp_krylov.cuh"
 #include "rp_mlp.cuh"
 #include "rp_vec.cuh"
@@ -25,6 +26,10 @@ struct rp_batch {
 
 struct rp_mlp {
     rp::Mlp net;
+};
+
+struct rp_dense {
+    rp::DenseSystem sys;
 };
 
 namespace rp {
@@ -142,6 +147,7 @@ int rp_shutdown(void) {
         workspace_release(g_ws);
         pipe_release();
         scratch_release_all();
+        dense_handles_release();
         if (g_dev_err) cudaFree(g_dev_err);
         g_dev_err = nullptr;
         if (g_stream) cudaStreamDestroy(g_stream);
@@ -765,6 +771,65 @@ int rp_batch_destroy(rp_batch_t b) {
         RP_CUDA(cudaStreamSynchronize(g_stream));
         batch_free(b->plan);
         delete b;
+    });
+}
+
+int rp_dense_create(rp_dense_t *d, int len, int dtype, uint64_t nterms, const uint64_t *bits,
+                    const double *coeff) {
+    return guarded([&] {
+        RP_REQUIRE(d, RP_E_INVALID, "null output pointer");
+        RP_REQUIRE(nterms < (1ull << 31), RP_E_INVALID, "too many terms");
+        rp_dense *D = new rp_dense;
+        try {
+            dense_build(D->sys, len, dtype, bits, coeff, (int64_t)nterms, g_stream);
+        } catch (...) {
+            delete D;
+            throw;
+        }
+        *d = D;
+    });
+}
+
+int rp_dense_eigenvalues(rp_dense_t d, double *evals) {
+    return guarded([&] {
+        RP_REQUIRE(d && evals, RP_E_INVALID, "null argument");
+        std::copy(d->sys.evals.begin(), d->sys.evals.end(), evals);
+    });
+}
+
+int rp_dense_eigenvector(rp_dense_t d, int64_t index, void *out) {
+    return guarded([&] {
+        RP_REQUIRE(d, RP_E_INVALID, "null argument");
+        check_vec(out);
+        dense_column(d->sys, index, out, g_stream);
+    });
+}
+
+int rp_dense_expm(rp_dense_t d, double cr, double ci, void *out) {
+    return guarded([&] {
+        RP_REQUIRE(d, RP_E_INVALID, "null argument");
+        check_vec(out);
+        dense_expm(d->sys, cr, ci, out, g_stream);
+    });
+}
+
+int rp_dense_destroy(rp_dense_t d) {
+    return guarded([&] {
+        if (!d) return;
+        RP_CUDA(cudaStreamSynchronize(g_stream));
+        dense_free(d->sys);
+        delete d;
+    });
+}
+
+int rp_mat_vec(int dtype, uint64_t dim, const void *mat, const void *vec, void *res) {
+    return guarded([&] {
+        check_dtype(dtype);
+        check_vec(mat);
+        check_vec(vec);
+        check_vec(res);
+        RP_REQUIRE(res != vec, RP_E_INVALID, "mat_vec needs distinct input and output vectors");
+        dense_matvec(dtype, dim, mat, vec, res, g_stream);
     });
 }
 

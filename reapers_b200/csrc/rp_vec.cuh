@@ -40,11 +40,13 @@ void multi_axpy(int dtype, uint64_t n, const VecTable &tab, int nvec, const int 
 void reduce_partials(const double *partials, int grid, int n, double *out, cudaStream_t st);
 
 // Device scratch kept between calls: the per-CTA partials of the one-off
-// inner product and norm, and the step-size candidates' expm buffer.  A slot
+// inner product and norm, the step-size candidates' expm buffer, the dense
+// matrix-vector product's column-chunk partials and the dense exponential's
+// scaled eigenvectors.  A slot
 // grows on demand (the stream is synchronised before a smaller buffer is
 // freed); scratch_release_all(), called by rp_shutdown, frees every slot, so
 // a later rp_init allocates them afresh.
-enum ScratchSlot { SCR_DOT = 0, SCR_NORM, SCR_EXPM, SCR_COUNT };
+enum ScratchSlot { SCR_DOT = 0, SCR_NORM, SCR_EXPM, SCR_MATVEC, SCR_EXPM_DENSE, SCR_COUNT };
 void *scratch_get(int slot, size_t bytes, cudaStream_t st);
 void scratch_release_all();
 

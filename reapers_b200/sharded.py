@@ -119,9 +119,10 @@ class ProcessGroupComm:
         """Every rank's device work issued so far is complete when this
         returns (the library stream and torch's are synchronised first)."""
         import torch
-        from . import synchronize
-        synchronize()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            from . import synchronize
+            synchronize()
+            torch.cuda.synchronize()
         self.dist.barrier(group=self.group)
         if self.dist.get_backend(self.group) == "nccl":
             torch.cuda.synchronize()

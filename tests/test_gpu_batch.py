@@ -130,3 +130,41 @@ def test_batched_row_tiles_match_tile_loop(cuda, team):
     for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
         ref = O.otoc(L, bits, coeff, w, v, psi, times, 12, 1e-12)
         assert np.abs(out[12][0][p] - ref).max() < 2e-5, (p, out[12][0][p], ref)
+
+
+def test_batch_with_single_path_problems_matches_oracle(cuda):
+    """Problems the autotuner sends to the single-problem path (path =
+    'single') run one at a time after the batched launches; the batch's
+    results keep the problems' order and match the oracle for both kinds."""
+    specs = [(16, 4), (20, 4), (18, 4), (20, 4)]
+    probs, refs = make_problems(specs, seed=21)
+    for i in (1, 3):
+        probs[i]["path"] = "single"
+    times = np.array([0.0, 0.7])
+    b = rb.BatchOTOC(probs, krydim=10, tol=1e-7, max_restarts=16)
+    F, ap = b.run(times)
+    b.close()
+    for p, (L, bits, coeff, w, v, psi) in enumerate(refs):
+        ref = O.otoc(L, bits, coeff, w, v, psi, times, 10, 1e-12)
+        assert np.abs(F[p] - ref).max() < 2e-5, (p, F[p], ref)
+        assert ap[p, 1] > 0
+
+
+def test_autotuner_picks_a_candidate_per_shape(cuda, tmp_path, monkeypatch):
+    """The tuner times one OTOC point for every candidate of a shape (the
+    batched launch per tile loop and team size, and the single-problem path)
+    and tags the problems with the fastest; a second call reads the cache."""
+    from reapers_b200 import autotune
+    monkeypatch.setenv("RPB200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    specs = [(28, 4)] * 3 + [(32, 4)] * 3
+    probs, _ = make_problems(specs, seed=40)
+    out = autotune.tune(probs, krydim=8, tol=1e-6, t_probe=0.3, nsingle=2)
+    assert len(out) >= 2
+    for rec in out.values():
+        assert autotune.SINGLE in rec["seconds"]
+        assert rec["path"] in ("batched", autotune.SINGLE)
+        assert min(rec["seconds"].values()) > 0
+    for p in probs:
+        assert p["path"] in ("batched", autotune.SINGLE)
+    again = autotune.tune(probs, krydim=8, tol=1e-6, t_probe=0.3, nsingle=2)
+    assert again == out

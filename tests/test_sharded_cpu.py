@@ -139,3 +139,75 @@ def test_xmask_split_matches_bits():
     parts = SH.shard_terms(L, k, bits, coeff, 0)
     assert sorted(parts) == sorted(set((S.xmask(bits) >> np.uint64(L - k)).astype(int).tolist()))
     assert sum(len(b) for b, _ in parts.values()) == len(bits)
+
+
+class _DenseFullOp(_DenseFull):
+    """The dense stand-in with the single-state apply too (test only)."""
+
+    def apply(self, out, inp, accumulate=False):
+        r = self.M @ inp
+        if accumulate:
+            out += r
+        else:
+            out.copy_(r)
+
+
+class _WallClock:
+    """Host timer standing in for the CUDA events of the GPU run (test only)."""
+
+    def start(self):
+        import time
+        self.t0 = time.perf_counter()
+
+    def stop(self):
+        import time
+        return time.perf_counter() - self.t0
+
+
+def _leg_worker(rank, world, port, L, bits, coeff, vec, out_dir):
+    import json
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        comm = SH.ProcessGroupComm()
+        out = bench.sharded_dist_leg(comm, L, bits, coeff, "c128", steps=2, warmup=1,
+                                     modes=("stage",), full=_DenseFullOp,
+                                     make_state=lambda: torch.from_numpy(vec.copy()),
+                                     clock=_WallClock())
+        if rank == 0:
+            with open(os.path.join(out_dir, "leg.json"), "w") as f:
+                json.dump(out, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_bench_sharded_leg_plumbing_over_gloo(world, tmp_path):
+    """bench.py's multi-GPU leg (the reference's high-bit split of one state
+    over the ranks) driven over a real gloo process group with the dense
+    stand-in operator and a host clock: every rank's output shard equals the
+    full product's, the partner shards the terms reach are the ones
+    exchanged, and rank 0 reports a time per apply for every rank."""
+    import json
+    L = 8
+    bits, coeff = random_terms(L, 50, seed=20 + world)
+    extra = np.array([(1 << (2 * (L - 1))) | 3, (3 << (2 * (L - 2)))], dtype=np.uint64)
+    bits = np.concatenate([bits, extra])
+    coeff = np.concatenate([coeff, [0.5, -1.25j]])
+    rng = np.random.default_rng(4)
+    vec = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    mp.spawn(_leg_worker, args=(world, _free_port(), L, bits, coeff, vec, str(tmp_path)),
+             nprocs=world, join=True)
+    leg = json.load(open(tmp_path / "leg.json"))
+    st = leg["modes"]["stage"]
+    assert st["bit_identical_to_full_apply"] is True
+    assert len(st["ms_per_apply_by_rank"]) == world
+    assert st["ms_per_apply"] == max(st["ms_per_apply_by_rank"])
+    k = world.bit_length() - 1
+    want = sorted(set((S.xmask(bits) >> np.uint64(L - k)).astype(int).tolist()) - {0})
+    assert st["partner_offsets"] == want
