@@ -226,6 +226,9 @@ int rp_dense_create(rp_dense_t *d, int len, int dtype, uint64_t nterms, const ui
                     const double *coeff);
 /* evals: 2^len doubles, ascending. */
 int rp_dense_eigenvalues(rp_dense_t d, double *evals);
+/* *mat = the device eigenvector matrix (2^len x 2^len, column-major, the
+ * dtype; owned by d, valid until rp_dense_destroy). */
+int rp_dense_eigenvectors(rp_dense_t d, void **mat);
 /* out (device vector, 2^len elements of the dtype) = eigenvector `index`:
  * the eigensystem column copy of ExactDiagonalization::ground_state. */
 int rp_dense_eigenvector(rp_dense_t d, int64_t index, void *out);
@@ -234,7 +237,7 @@ int rp_dense_eigenvector(rp_dense_t d, int64_t index, void *out);
 int rp_dense_expm(rp_dense_t d, double cr, double ci, void *out);
 int rp_dense_destroy(rp_dense_t d);
 /* res = mat vec for a dense dim x dim column-major device matrix
- * (GPUImpl::mat_mul, inc/gpuimpl.h:1003-1021): FP64 accumulation, fixed
+ * (GPUImpl::mat_mul, inc/gpuimpl.h:1012-1021): FP64 accumulation, fixed
  * summation order; res and vec distinct. */
 int rp_mat_vec(int dtype, uint64_t dim, const void *mat, const void *vec, void *res);
 

@@ -19,9 +19,11 @@
  *
  * Link with -lrpb200.  Vectors live in device memory; element access goes
  * through a proxy that copies one element (as GPUImpl's DeviceVec does).
- * Dense-matrix members of the concept (mat_mul, the eigen-system copy_vec)
- * are not provided: they belong to exact diagonalisation, which is not on
- * this path.
+ * Exact diagonalisation (ExactDiagonalization<B200Impl>, inc/algo.h:29-54)
+ * runs on the device as on the reference's GPU backend: B200SumOps builds
+ * the dense matrix and its eigensystem (rp_dense_*), matexp results are
+ * device matrices kept in the reference's own MatexpCache, and B200Impl's
+ * mat_mul and eigenvector copy_vec work on them.
  */
 #pragma once
 
@@ -31,7 +33,9 @@
 
 #include <complex>
 #include <cstdint>
+#include <memory>
 #include <random>
+#include <tuple>
 #include <string>
 #include <type_traits>
 #include <utility>
@@ -156,25 +160,122 @@ public:
     std::size_t dimension() const { return dim; }
 };
 
+/* A dense complex matrix in device memory, column-major (the role of
+ * DevSumOps::MatrixType, inc/gpuimpl.h:139-300): matexp results and the
+ * eigenvector matrix.  A view does not own its memory (the eigenvectors of
+ * an rp_dense_t); copies are owning device copies. */
+template <RealScalar FpType>
+class B200Mat {
+    std::size_t rdim = 0, cdim = 0;
+    void *p = nullptr;
+    bool owns = false;
+
+public:
+    B200Mat() = default;
+    B200Mat(std::size_t rows, std::size_t cols) : rdim(rows), cdim(cols), owns(true) {
+        const std::size_t b = rows * cols * sizeof(complex<FpType>);
+        b200::check(rp_alloc(&p, b), b);
+    }
+    static B200Mat view(void *ptr, std::size_t rows, std::size_t cols) {
+        B200Mat m;
+        m.rdim = rows;
+        m.cdim = cols;
+        m.p = ptr;
+        return m;
+    }
+    B200Mat(const B200Mat &o) : B200Mat(o.rdim, o.cdim) {
+        if (size()) b200::check(rp_memcpy(p, o.p, size() * sizeof(complex<FpType>), 2));
+    }
+    B200Mat(B200Mat &&o) noexcept : rdim(o.rdim), cdim(o.cdim), p(o.p), owns(o.owns) {
+        o.p = nullptr;
+        o.owns = false;
+        o.rdim = o.cdim = 0;
+    }
+    B200Mat &operator=(B200Mat o) noexcept {
+        std::swap(rdim, o.rdim);
+        std::swap(cdim, o.cdim);
+        std::swap(p, o.p);
+        std::swap(owns, o.owns);
+        return *this;
+    }
+    ~B200Mat() {
+        if (owns && p) rp_free(p);
+    }
+    std::size_t rows() const { return rdim; }
+    std::size_t cols() const { return cdim; }
+    /* elements (MatexpCache accounts sizeof(complex) * size() bytes) */
+    std::size_t size() const { return rdim * cdim; }
+    void *ptr() const { return p; }
+};
+
 /* A sum of spin operators whose device table (grouped terms) is built on the
  * first apply and dropped on every change, as DevSumOps does with its device
  * copy (inc/gpuimpl.h:124-395, upload/release at 1065-1105). */
 template <RealScalar FpType>
 class B200SumOps : public HostSumOps<FpType> {
     friend class B200Impl;
+    friend class HostSumOps<FpType>;   // its _matexp_helper reads our cache
+    using Impl = B200Impl;
+
+public:
+    using MatrixType = B200Mat<FpType>;
+    using EigenVals = typename HostSumOps<FpType>::EigenVals;
+    using EigenVecs = B200Mat<FpType>;
+    using EigenSystem = std::tuple<const EigenVals &, const EigenVecs &>;
+
+private:
     mutable rp_ham_t ham = nullptr;
     mutable int ham_len = -1;
+    // exact diagonalisation: the device eigensystem and the matexp results
+    mutable rp_dense_t dense = nullptr;
+    mutable int dense_len = -1;
+    mutable EigenVals dense_evals;
+    mutable EigenVecs dense_vecs;
+    mutable MatexpCache<FpType, MatrixType, B200Impl> matexp_cache;
 
     void drop() const {
         if (ham) rp_ham_destroy(ham);
         ham = nullptr;
         ham_len = -1;
+        matexp_cache.clear();
+        dense_vecs = EigenVecs();
+        if (dense) rp_dense_destroy(dense);
+        dense = nullptr;
+        dense_len = -1;
+    }
+
+    /* bit strings and the coefficients the kernels take (sigma_y as sx.sz
+     * with its i in the coefficient, inc/ops.h:285-288 and 366-377) */
+    void term_arrays(std::vector<uint64_t> &bits, std::vector<double> &coeff) const {
+        for (const auto &op : *this) {
+            const uint64_t b = (uint64_t)op.get_bit_string();
+            const uint64_t xb = b & 0x5555555555555555ull, zb = (b >> 1) & 0x5555555555555555ull;
+            const int ny = __builtin_popcountll(xb & zb) & 3;
+            std::complex<double> c(op.coefficient().real(), op.coefficient().imag());
+            static const std::complex<double> ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+            c *= ipow[ny];
+            bits.push_back(b);
+            coeff.push_back(c.real());
+            coeff.push_back(c.imag());
+        }
+    }
+
+    /* exp(c H) on the device (DevSumOps::_matexp, inc/gpuimpl.h:1244-1263) */
+    MatrixType _matexp(complex<FpType> c, int len) const {
+        get_eigensystem(len);
+        MatrixType res(dense_vecs.rows(), dense_vecs.cols());
+        b200::check(rp_dense_expm(dense, (double)c.real(), (double)c.imag(), res.ptr()));
+        return res;
     }
 
 protected:
     void release() const override {
         drop();
         HostSumOps<FpType>::release();
+    }
+    void mini_release() const override {
+        matexp_cache.clear();
+        HostSumOps<FpType>::mini_release();
     }
 
 public:
@@ -196,31 +297,58 @@ public:
     }
     ~B200SumOps() { drop(); }
 
-    /* The library's grouped term table for a chain of len sites: the stored
-     * bit strings and coefficients (sigma_y as sx.sz with its i in the
-     * coefficient, inc/ops.h:285-288 and 366-377). */
+    /* The library's grouped term table for a chain of len sites. */
     rp_ham_t handle(int len) const {
         if (ham && ham_len == len) return ham;
-        drop();
+        if (ham) rp_ham_destroy(ham);
+        ham = nullptr;
+        ham_len = -1;
         std::vector<uint64_t> bits;
         std::vector<double> coeff;
-        for (const auto &op : *this) {
-            const uint64_t b = (uint64_t)op.get_bit_string();
-            const uint64_t xb = b & 0x5555555555555555ull, zb = (b >> 1) & 0x5555555555555555ull;
-            const int ny = __builtin_popcountll(xb & zb) & 3;
-            std::complex<double> c(op.coefficient().real(), op.coefficient().imag());
-            static const std::complex<double> ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
-            c *= ipow[ny];
-            bits.push_back(b);
-            coeff.push_back(c.real());
-            coeff.push_back(c.imag());
-        }
+        term_arrays(bits, coeff);
         rp_ham_t h = nullptr;
         b200::check(rp_ham_create(&h, len, b200::code<FpType>(), bits.size(), bits.data(),
                                   coeff.data()));
         ham = h;
         ham_len = len;
         return ham;
+    }
+
+    /* The eigensystem of the (Hermitian) operator on len sites, computed on
+     * the device once per len (DevSumOps::get_eigensystem,
+     * inc/gpuimpl.h:1180-1240): eigenvalues ascending on the host, the
+     * eigenvectors the columns of a device matrix. */
+    EigenSystem get_eigensystem(int len) const {
+        if (!dense || dense_len != len) {
+            matexp_cache.clear();
+            dense_vecs = EigenVecs();
+            if (dense) rp_dense_destroy(dense);
+            dense = nullptr;
+            dense_len = -1;
+            std::vector<uint64_t> bits;
+            std::vector<double> coeff;
+            term_arrays(bits, coeff);
+            rp_dense_t d = nullptr;
+            b200::check(rp_dense_create(&d, len, b200::code<FpType>(), bits.size(), bits.data(),
+                                        coeff.data()));
+            dense = d;
+            dense_len = len;
+            const std::size_t dim = std::size_t(1) << len;
+            std::vector<double> ev(dim);
+            b200::check(rp_dense_eigenvalues(dense, ev.data()));
+            dense_evals.resize(dim, 1);
+            for (std::size_t i = 0; i < dim; i++) dense_evals(i, 0) = (FpType)ev[i];
+            void *vp = nullptr;
+            b200::check(rp_dense_eigenvectors(dense, &vp));
+            dense_vecs = EigenVecs::view(vp, dim, dim);
+        }
+        return {dense_evals, dense_vecs};
+    }
+
+    /* exp(c H) for a chain of len sites, kept in the reference's MatexpCache
+     * (inc/cpuimpl.h:25-88) by its HostSumOps::_matexp_helper. */
+    const MatrixType &matexp(complex<FpType> c, int len) const {
+        return HostSumOps<FpType>::_matexp_helper(*this, c, len);
     }
 };
 
@@ -304,6 +432,47 @@ public:
         double n = 0;
         b200::check(rp_vec_norm(b200::code<FpType>(), size, v.ptr(), &n));
         return FpType(n);
+    }
+
+    /* res = mat * vec for a device matrix (GPUImpl::mat_mul,
+     * inc/gpuimpl.h:1012-1021; ExactDiagonalization::evolve) */
+    template <RealScalar FpType>
+    static void mat_mul(VecSizeType<FpType> dim, BufType<FpType> res, const B200Mat<FpType> &mat,
+                        ConstBufType<FpType> vec) {
+        if (mat.rows() != dim || mat.cols() != dim)
+            throw InvalidArgument(__FILE__, __LINE__, __func__, "matrix and vector sizes differ");
+        b200::check(rp_mat_vec(b200::code<FpType>(), dim, mat.ptr(), vec.ptr(), res.ptr()));
+    }
+
+    /* res = column col of a device matrix (the eigenvector copy of
+     * ExactDiagonalization::ground_state; GPUImpl::copy_vec,
+     * inc/gpuimpl.h:894-900) */
+    template <RealScalar FpType>
+    static void copy_vec(VecSizeType<FpType> size, BufType<FpType> res, const B200Mat<FpType> &mat,
+                         ssize_t col) {
+        if (col < 0 || (std::size_t)col >= mat.cols() || mat.rows() != size)
+            throw InvalidArgument(__FILE__, __LINE__, __func__, "eigenvector index out of range");
+        const std::size_t b = size * sizeof(complex<FpType>);
+        b200::check(rp_memcpy(res.ptr(), static_cast<char *>(mat.ptr()) + (std::size_t)col * b, b, 2));
+    }
+
+    /* Device memory budget of the matexp cache (the reference's
+     * cache_reserve / cache_release / set_max_cache_size, inc/gpuimpl.h:560-590). */
+    inline static std::size_t max_cache_size = std::size_t(16) << 30;
+    inline static std::size_t cache_size = 0;
+    static bool cache_reserve(std::size_t sz) {
+        if (cache_size + sz > max_cache_size) return false;
+        cache_size += sz;
+        return true;
+    }
+    static void cache_release(std::size_t sz) { cache_size -= sz <= cache_size ? sz : cache_size; }
+    static void set_max_cache_size(std::size_t sz) { max_cache_size = sz; }
+    static std::size_t get_max_cache_size() { return max_cache_size; }
+    static std::size_t get_current_cache_size() { return cache_size; }
+    static int get_device_count() {
+        int n = 0;
+        b200::check(rp_device_count(&n));
+        return n;
     }
 
     /* res += ops * vec (inc/cpuimpl.h:738-754, src/krnl.cu:220-257) */

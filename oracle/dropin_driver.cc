@@ -157,6 +157,36 @@ int main(int argc, char **argv) {
     CSt ggh(gg);
     const double overlap = std::abs(gc * ggh);
 
+    // exact diagonalisation (inc/algo.h:29-54) on both backends: B200Impl's
+    // eigensystem, matexp and mat_mul run on the device (rp_dense_*); the
+    // CPU backend's eigen solve (the Eigen-API subset's Jacobi method) runs
+    // only up to 2^8 states, above that the references are the CPU backend's
+    // Lanczos ground state and restarted Krylov evolve
+    GSt eg(L);
+    const double Eed = eg.template ground_state<ExactDiagonalization>(ham_g);
+    CSt egh(eg);
+    const double ed_overlap = std::abs(gc * egh);
+    GSt ee(g0);
+    ee.template evolve<ExactDiagonalization>(ham_g, t, 0.0);
+    const double ed_evolve = rel_diff(ee, c2);
+    GSt ee2(g0);
+    ee2.template evolve<ExactDiagonalization>(ham_g, t, 0.0);   // the matexp cache's hit
+    const double ed_cached = rel_diff(ee2, c2);
+    const double ed_cache_bytes = (double)B200Impl::get_current_cache_size();
+    GSt eb(g0);
+    eb.template evolve<ExactDiagonalization>(ham_g, 0.3 * t, 0.2);
+    const double ed_beta = rel_diff(eb, c4);
+    double ed_cpu_energy = 0.0, ed_cpu_evolve = 0.0;
+    int ed_cpu = 0;
+    if (L <= 8) {
+        CSt ec(L);
+        ed_cpu_energy = ec.template ground_state<ExactDiagonalization>(ham_c);
+        CSt ev(c0);
+        ev.template evolve<ExactDiagonalization>(ham_c, t, 0.0);
+        ed_cpu_evolve = rel_diff(ee, ev);
+        ed_cpu = 1;
+    }
+
     // parity-block form (FermionOpBlockForm, BlockDiag, BlockState): the
     // OTOC of examples/syk.cc (OTOC::evolve at beta = 0) on one block of
     // N/2 - 1 qubits, and a BlockState evolved under BlockDiag(H_LL, H_RR)
@@ -209,6 +239,12 @@ int main(int argc, char **argv) {
         "{\"block_terms\": %.3e, \"otoc_block\": %.3e, \"F_block\": [%.12e, %.12e], "
         "\"block_evolve\": %.3e, ", bterms, otoc_block, (double)Fbc.real(), (double)Fbc.imag(),
         block_evolve);
+    std::printf(
+        "\"E0_ed_b200\": %.15e, \"ed_overlap\": %.15f, \"ed_evolve\": %.3e, "
+        "\"ed_evolve_cached\": %.3e, \"ed_cache_bytes\": %.0f, \"ed_beta\": %.3e, "
+        "\"ed_cpu\": %d, \"E0_ed_cpu\": %.15e, \"ed_vs_cpu_ed\": %.3e, ",
+        Eed, ed_overlap, ed_evolve, ed_cached, ed_cache_bytes, ed_beta, ed_cpu, ed_cpu_energy,
+        ed_cpu_evolve);
     std::printf(
         "\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
         "\"apply\": %.3e, \"evolve_ref_krylov\": %.3e, \"evolve_b200krylov\": %.3e, "

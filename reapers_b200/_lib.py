@@ -95,6 +95,7 @@ _SIGS = {
                                   C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "rp_dense_eigenvalues": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "rp_dense_eigenvector": (C.c_int, [_VP, C.c_int64, _VP]),
+    "rp_dense_eigenvectors": (C.c_int, [_VP, C.POINTER(_VP)]),
     "rp_dense_expm": (C.c_int, [_VP, C.c_double, C.c_double, _VP]),
     "rp_dense_destroy": (C.c_int, [_VP]),
     "rp_mat_vec": (C.c_int, [C.c_int, C.c_uint64, _VP, _VP, _VP]),

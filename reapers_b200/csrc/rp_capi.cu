@@ -797,6 +797,13 @@ int rp_dense_eigenvalues(rp_dense_t d, double *evals) {
     });
 }
 
+int rp_dense_eigenvectors(rp_dense_t d, void **mat) {
+    return guarded([&] {
+        RP_REQUIRE(d && mat, RP_E_INVALID, "null argument");
+        *mat = d->sys.evecs;
+    });
+}
+
 int rp_dense_eigenvector(rp_dense_t d, int64_t index, void *out) {
     return guarded([&] {
         RP_REQUIRE(d, RP_E_INVALID, "null argument");

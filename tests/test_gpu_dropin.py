@@ -10,9 +10,11 @@ GPU-resident Krylov selected as State::evolve<B200Krylov>, imaginary-time
 evolution, the OTOC sequence of examples/simple-syk-krylov.cc, an apply
 after the operator is changed (device table dropped and rebuilt), and the
 reference's ground-state Lanczos (energy; state overlap where the ground
-state is not degenerate); and the parity-block form (FermionOpBlockForm,
-BlockDiag, BlockState): block term lists, the OTOC sequence of
-examples/syk.cc on one block, a block state evolve.
+state is not degenerate); the reference's exact diagonalisation
+(ExactDiagonalization: eigensystem, matexp cache, mat_mul and the
+eigenvector copy on the device); and the parity-block form
+(FermionOpBlockForm, BlockDiag, BlockState): block term lists, the OTOC
+sequence of examples/syk.cc on one block, a block state evolve.
 """
 import json
 import os
@@ -36,6 +38,8 @@ def test_dropin_driver_is_built_against_librpb200():
     (16, 0.0, 3, 1.0, 8),      # dense SYK, 1820 terms >= 2^8: the reference takes its dense path
     (20, 8.0, 5, 2.0, 10),     # sparse SYK k = 8
     (24, 8.0, 7, 1.5, 12),     # sparse SYK, 12 qubits
+    (24, 0.0, 1, 1.0, 20),     # dense SYK N = 24 (10626 terms, 12 qubits): the exact
+                               # diagonalisation shape of the small-N dense path
 ])
 def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
     r = subprocess.run([DRIVER, str(N), str(sp), str(seed), str(t), str(krydim)],
@@ -55,3 +59,17 @@ def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
     assert abs(d["E0_b200"] - d["E0_cpu"]) <= 1e-10 * abs(d["E0_cpu"]), d
     if N % 8 == 0:   # no parity-sector degeneracy: the same state up to a phase
         assert d["ground_overlap"] >= 1 - 1e-8, d
+    # exact diagonalisation (inc/algo.h:29-54) on B200Impl: the device
+    # eigensystem's ground energy against the CPU backend's Lanczos, the
+    # matexp evolve (and its cached repeat, and imaginary time) against the
+    # CPU backend's restarted Krylov; up to 2^8 states also against the CPU
+    # backend's own exact diagonalisation
+    assert abs(d["E0_ed_b200"] - d["E0_cpu"]) <= 1e-9 * abs(d["E0_cpu"]), d
+    if N % 8 == 0:
+        assert d["ed_overlap"] >= 1 - 1e-8, d
+    assert d["ed_evolve"] <= 1e-10 and d["ed_evolve_cached"] <= 1e-10, d
+    assert d["ed_cache_bytes"] > 0, d
+    assert d["ed_beta"] <= 1e-10, d
+    if d["ed_cpu"]:
+        assert abs(d["E0_ed_cpu"] - d["E0_ed_b200"]) <= 1e-10 * abs(d["E0_ed_cpu"]), d
+        assert d["ed_vs_cpu_ed"] <= 1e-10, d

@@ -276,10 +276,11 @@ def test_apply_host_pipeline_matches_device_apply(dtype, L):
 @pytest.mark.gpu
 def test_dense_path_matches_krylov_on_dense_syk_n24():
     """Exact diagonalisation (inc/algo.h:27-54) on the GPU for the dense SYK
-    of 12 qubits (all 10626 quartets of N = 24): the matrix equals the
-    oracle's, exp(-iHt) psi equals the oracle's restarted Krylov at
-    t = 0.5 .. 5 (tol 1e-12), exponentials are cached per exponent, and the
-    ground state is the lowest eigenpair."""
+    of 12 qubits (all 10626 quartets of N = 24), through the library's dense
+    path (rp_dense_*): V diag(lambda) V^H rebuilds the oracle's matrix, the
+    eigenvalues are the oracle's, exp(-iHt) psi equals the oracle's
+    restarted Krylov at t = 0.5 .. 5 (tol 1e-12), exponentials are cached
+    per exponent, and the ground state is the lowest eigenpair."""
     import reapers_b200 as rb
     from reapers_b200.dense import DenseEvolver
     from oracle import oracle as O
@@ -288,7 +289,10 @@ def test_dense_path_matches_krylov_on_dense_syk_n24():
     ham = rb.Hamiltonian(L, bits, coeff, "c128")
     ev = DenseEvolver(ham)
     Hd = O.dense_matrix(L, bits, coeff)
-    assert np.abs(ev.matrix().cpu().numpy() - Hd).max() <= 1e-13 * np.abs(Hd).max()
+    lam = ev.eigenvalues()
+    V = ev.eigenvectors().cpu().numpy()
+    assert np.abs(lam - np.linalg.eigvalsh(Hd)).max() <= 1e-12 * np.abs(lam).max()
+    assert np.abs((V * lam) @ V.conj().T - Hd).max() <= 1e-11 * np.abs(Hd).max()
     rng = np.random.default_rng(7)
     psi0 = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
     psi0 /= np.linalg.norm(psi0)
@@ -304,6 +308,49 @@ def test_dense_path_matches_krylov_on_dense_syk_n24():
     assert abs(E0 - np.linalg.eigvalsh(Hd)[0]) <= 1e-10
     gv = g.cpu().numpy()
     assert np.linalg.norm(Hd @ gv - E0 * gv) <= 1e-9
+    ev.close()
+    ham.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["c64", "c128"])
+def test_dense_entry_points_small(dtype):
+    """rp_dense_* and rp_mat_vec on a random Hermitian Pauli sum of 7 qubits
+    (complex and Y-carrying coefficients) against numpy: eigenvalues, the
+    exponential exp(c H) for a complex c, and the matrix-vector product;
+    FP64 to 1e-12, FP32 to 1e-5 relative."""
+    import reapers_b200 as rb
+    from reapers_b200.dense import DenseEvolver
+    from oracle import oracle as O
+    from scipy.linalg import expm
+    L = 7
+    rng = np.random.default_rng(9)
+    bits = np.unique(rng.integers(0, 1 << (2 * L), 40, dtype=np.uint64))
+    # Hermitian: a Pauli string times a real number, sigma_y's i carried by
+    # the stored coefficient (i^(number of Y factors))
+    x = np.array([int(b) & 0x5555 for b in bits], dtype=np.int64)
+    z = np.array([(int(b) >> 1) & 0x5555 for b in bits], dtype=np.int64)
+    ny = np.array([bin(int(a) & int(c)).count("1") for a, c in zip(x, z)])
+    coeff = rng.standard_normal(len(bits)) * (1j ** ny)
+    Hd = O.dense_matrix(L, bits, coeff)
+    assert np.abs(Hd - Hd.conj().T).max() < 1e-14
+    tol = 1e-12 if dtype == "c128" else 1e-5
+    ham = rb.Hamiltonian(L, bits, coeff, dtype)
+    ev = DenseEvolver(ham)
+    lam = ev.eigenvalues()
+    ref = np.linalg.eigvalsh(Hd)
+    assert np.abs(lam - ref).max() <= tol * np.abs(ref).max() * 10
+    c = complex(-0.3, -1.7)
+    E = ev.matexp(c).cpu().numpy().reshape(1 << L, 1 << L).T
+    Er = expm(c * Hd)
+    assert np.abs(E - Er).max() <= tol * np.abs(Er).max() * 10
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    tdt = torch.complex64 if dtype == "c64" else torch.complex128
+    xg = torch.from_numpy(psi).to(tdt).cuda()
+    ev.evolve(xg, 1.7, 0.3)
+    want = Er @ psi
+    assert np.linalg.norm(xg.cpu().numpy() - want) <= tol * np.linalg.norm(want) * 10
+    ev.close()
     ham.close()
 
 
