@@ -213,6 +213,45 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16, last=True):
     return out
 
 
+def otoc_full_leg(cfg, nreal, nstates, krydim=16, npts=20, seed0=1000):
+    """The N = 56 OTOC workload as stated: nreal disorder realisations x
+    nstates random states, F(t) at all `npts` points of the grid on [0, 15],
+    m = 16, in the plain FP64 path and the mixed path, through otoc_leg's
+    sequence (W = b_{N-1}, V = b_{N-2}).  Reports the time of both paths over
+    the whole set, the speed-up, and the largest |F_mixed - F_fp64| / |F(0)|
+    over every problem and point."""
+    import reapers_b200 as rb
+    out = {"workload": f"sparse SYK N={cfg['N']} (2^{cfg['N'] // 2}), k={cfg['k']}, {nreal} "
+                       f"realisations x {nstates} states, {npts} points on [0, 15], m={krydim}",
+           "problems": []}
+    tot = {"fp64_plain": 0.0, "mixed_fp32": 0.0}
+    err = 0.0
+    for r in range(nreal):
+        bits, coeff = rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed0 + r)
+        for st in range(nstates):
+            leg = otoc_leg(cfg, bits, coeff, seed=7 + 31 * r + st, npts=npts - 1, krydim=krydim,
+                           last=False)
+            for k in tot:
+                tot[k] += leg[k]["seconds"]
+            err = max(err, leg["mixed_max_rel_err_vs_fp64"])
+            out["problems"].append({"realisation": r, "state": st,
+                                    "fp64_seconds": leg["fp64_plain"]["seconds"],
+                                    "mixed_seconds": leg["mixed_fp32"]["seconds"],
+                                    "fp64_applies": leg["fp64_plain"]["applies"],
+                                    "mixed_applies": leg["mixed_fp32"]["applies"],
+                                    "max_rel_err": leg["mixed_max_rel_err_vs_fp64"],
+                                    "rel_err_per_point": leg["mixed_rel_err_per_point"],
+                                    "F_fp64": leg["fp64_plain"]["F"]})
+    npoints = nreal * nstates * (npts - 1)
+    out["fp64_plain"] = {"seconds": round(tot["fp64_plain"], 2),
+                         "pts_per_s": round(npoints / tot["fp64_plain"], 5)}
+    out["mixed_fp32"] = {"seconds": round(tot["mixed_fp32"], 2),
+                         "pts_per_s": round(npoints / tot["mixed_fp32"], 5)}
+    out["speedup_mixed_vs_fp64"] = round(tot["fp64_plain"] / tot["mixed_fp32"], 3)
+    out["mixed_max_rel_err_vs_fp64"] = err
+    return out
+
+
 def evolve_leg(seed=0, t=10.0, krydim=30, cpu=True):
     """exp(-iHt) psi for sparse SYK N = 48 (24 qubits, k = 8, 384 terms),
     one random state, m = 30, t = 10: the plain FP64 path (tol = FP64
@@ -545,6 +584,20 @@ def batch_leg(seed=0, points=(1, 2, 20, 39), krydim=16, nreal=64, nstates=8,
     out["per_size_best_pts_per_s"] = round(pts / tot_best, 3)
     out["speedup_batched_vs_sequential"] = round(tot_seq / tot_batch, 3)
     out["max_abs_diff_batched_vs_sequential"] = err
+    # the whole batch at once, every size in one persistent launch per time
+    # step and team size (largest problems first from the shared queue, the
+    # smaller ones filling teams as they free up), the single-path shapes
+    # after it
+    b = rb.BatchOTOC(problems, krydim=krydim, tol=tol, max_restarts=16)
+    b.run(times[:1], use_graph=True)    # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F_all, _ = b.run(times, use_graph=True)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    b.close()
+    out["whole_batch_one_launch"] = {"seconds": round(el, 3), "pts_per_s": round(pts / el, 3),
+                                     "speedup_vs_sequential": round(tot_seq / el, 3)}
     out["launches_per_time_step"] = 1
     out["cuda_graph"] = True
     return out
@@ -622,6 +675,33 @@ def step_leg(T=10.0, tol=1e-8, seed=0):
     out["speedup_wall_total"] = round(tot["plain"][1] / tot["learned"][1], 3)
     out["speedup_wall_total_vs_stretch"] = round(tot["plain+stretch"][1] / tot["learned"][1], 3)
     return out
+
+
+def gpu_reference_leg(cfg, bits, coeff, t_ours, reps=3):
+    """The reference's own GPU kernel (krnl_apply_ops, one thread per element,
+    src/krnl.cu:81-94, launched by GPUImpl::apply_ops, src/krnl.cu:220-257),
+    compiled for sm_100a from its sources (oracle/_ref/ref_gpu_driver), timed on
+    the same Hamiltonian and state size on this GPU with CUDA events: a
+    GPU-side baseline beside the CPU one.  Its results equal the product's
+    (tests/test_gpu_ref_kernel.py)."""
+    from oracle import oracle as O
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_driver")
+    if not os.path.exists(drv):
+        return {"unavailable": "oracle/_ref/ref_gpu_driver was not built"}
+    L = cfg["N"] // 2
+    tmp = tempfile.mkdtemp(prefix="rpgpu_")
+    tf = os.path.join(tmp, "terms")
+    O.write_terms(tf, L, bits, coeff)
+    fp = "32" if cfg["dtype"] == "c64" else "64"
+    r = subprocess.run([drv, "bench", tf, fp, str(reps)], capture_output=True, text=True,
+                       timeout=900)
+    if r.returncode != 0:
+        return {"failed": r.stderr[-300:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"kernel": "reference krnl_apply_ops (GPUImpl), sm_100a build of src/krnl.cu",
+            "ms_per_apply": d["ms_per_apply"], "reps": reps,
+            "ours_ms_per_apply": round(t_ours * 1e3, 3),
+            "speedup_ours_vs_reference_gpu": round(d["ms_per_apply"] / (t_ours * 1e3), 2)}
 
 
 def make_terms(cfg, seed):
@@ -811,16 +891,23 @@ def run_ours(args):
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
+    if legs and not args.no_refgpu:
+        line["gpu_reference_kernel"] = gpu_reference_leg(cfg, bits, coeff, t_step)
     if legs and args.config == "syk56" and not args.no_chains:
         line["hpsi_spin_chains_l28"] = spin_chain_leg(clocks)
     # the sharded leg uses this leg's Hamiltonian and state, so it runs
     # before the OTOC leg frees them
     if legs and args.config == "syk56" and not args.no_shard:
         line["sharded_peer_syk56"] = shard_leg(ham, x, L)
-    if legs and args.config == "syk56" and not args.no_otoc:
+    if legs and args.config == "syk56" and (not args.no_otoc or args.otoc_full):
+        ham.close()
         del x, ham
         torch.cuda.empty_cache()
+    if legs and args.config == "syk56" and not args.no_otoc:
         line["otoc"] = otoc_leg(cfg, bits, coeff, seed=7 + rank, npts=args.otoc_points)
+    if legs and args.config == "syk56" and args.otoc_full:
+        nr, ns = (int(v) for v in args.otoc_full.split("x"))
+        line["otoc_full"] = otoc_full_leg(cfg, nr, ns)
     if legs and args.config == "syk56" and not args.no_evolve:
         line["evolve_syk48"] = evolve_leg(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
     if legs and args.config == "syk56" and not args.no_batch:
@@ -920,12 +1007,17 @@ def main():
     ap.add_argument("--no-shard", action="store_true",
                     help="skip the peer-read sharded H.psi leg (virtual shards on one GPU)")
     ap.add_argument("--no-otoc", action="store_true", help="skip the N=56 OTOC leg")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip the reference's own GPU kernel (sm_100a build) timed beside ours")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched OTOC leg (sparse SYK N = 32/36/40)")
     ap.add_argument("--no-evolve", action="store_true", help="skip the N = 48 FP64 vs mixed evolve leg")
     ap.add_argument("--no-steps", action="store_true",
                     help="skip the learned step-controller leg")
     ap.add_argument("--otoc-points", type=int, default=2,
                     help="non-zero time points of the 20-point grid on [0, 15] in the N = 56 OTOC sample")
+    ap.add_argument("--otoc-full", default="",
+                    help="RxS: also run the N = 56 OTOC on R realisations x S states at all 20 "
+                         "points in both precisions (e.g. 4x2; minutes per problem)")
     ap.add_argument("--profile", action="store_true",
                     help="run two applies and exit (for an ncu capture)")
     args = ap.parse_args()

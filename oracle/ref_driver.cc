@@ -31,6 +31,8 @@ using namespace REAPERS;
 using namespace REAPERS::Model;
 using namespace REAPERS::EvolutionAlgorithm;
 
+#include "ref_io.h"
+
 // CPUImpl with call counters, so that the number of H.psi products and inner
 // products of a reference evolve can be compared with the oracle's.
 struct CountingImpl : CPUImpl {
@@ -57,21 +59,8 @@ struct CountingImpl : CPUImpl {
 using Ops = HostSumOps<double>;
 using St = State<double, CountingImpl>;
 
-struct Term { uint64_t bits; double re, im; };
-
 static double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
-static std::vector<Term> read_terms(const char *path, int &len) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) { std::cerr << "cannot open " << path << "\n"; exit(2); }
-    int64_t T; int32_t l;
-    f.read((char *)&T, 8); f.read((char *)&l, 4);
-    std::vector<Term> t(T);
-    f.read((char *)t.data(), T * sizeof(Term));
-    len = l;
-    return t;
 }
 
 static void write_records(std::ofstream &f, const Ops &ops) {
@@ -96,28 +85,6 @@ static void write_terms(const char *path, const Ops &ops, int len) {
     int64_t T = ops.size(); int32_t l = len;
     f.write((const char *)&T, 8); f.write((const char *)&l, 4);
     write_records(f, ops);
-}
-
-// Build a SpinOp with the given internal bits and stored coefficient through
-// the public API: right-multiply single-site sigma matrices (no carry-over
-// sign arises between different sites), then fix the coefficient.
-template <typename Fp>
-static SpinOp<Fp> make_op(const Term &t) {
-    auto op = SpinOp<Fp>::identity();
-    for (int i = 0; i < 32; i++) {
-        unsigned s = (t.bits >> (2 * i)) & 3;
-        if (s == 1) op *= SpinOp<Fp>::sigma_x(i);
-        else if (s == 2) op *= SpinOp<Fp>::sigma_z(i);
-        else if (s == 3) op *= SpinOp<Fp>::sigma_y(i);
-    }
-    // the coefficient is now i^ny; multiply by target * conj(i^ny) (exact)
-    int ny = 0;
-    for (int i = 0; i < 32; i++) if (((t.bits >> (2 * i)) & 3) == 3) ny++;
-    std::complex<double> cur(1, 0);
-    for (int k = 0; k < (ny & 3); k++) cur *= std::complex<double>(0, 1);
-    std::complex<double> f = std::complex<double>(t.re, t.im) * std::conj(cur);
-    op *= complex<Fp>((Fp)f.real(), (Fp)f.imag());
-    return op;
 }
 
 template <typename Fp = double>

@@ -69,12 +69,13 @@ def shape_key(prob, krydim):
 def candidates(L):
     """(B, C) pairs of the batched launch tried for L qubits: every tile
     exponent and team size below 2^14 elements; from there the row-tile loop
-    (B = 12), with one CTA per problem dropped from 2^16 elements on (a
-    problem's Krylov vectors then stream through one SM)."""
+    (B = 12) with teams of 1 to 8 CTAs (on the B200, timed by whole OTOC
+    points, teams of 16 never won from 2^16 elements on: the cluster
+    barriers and the leader's expm cost more than the bandwidth they add)."""
     if L < 14:
         return [(B, C) for B in range(8, min(12, L) + 1) for C in (1, 2, 4, 8, 16)
                 if C <= (1 << (L - B))]
-    teams = (1, 2, 4, 8, 16) if L < 16 else (2, 4, 8, 16)
+    teams = (1, 2, 4, 8, 16) if L < 16 else (1, 2, 4, 8)
     return [(12, C) for C in teams if C <= (1 << (L - 12))]
 
 
@@ -115,7 +116,7 @@ def _time_single(probs, krydim, tol, t_probe, nsingle):
                 x.close()
 
 
-def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, t_probe=0.5, sample=None,
+def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, t_probe=0.3, sample=None,
          nsingle=4, force=False, log=None):
     """Set problems[i]['tile'] / ['team'] to the tuned pair, or
     problems[i]['path'] = 'single'; returns {key: record}."""
