@@ -69,13 +69,16 @@ def shape_key(prob, krydim):
 def candidates(L):
     """(B, C) pairs of the batched launch tried for L qubits: every tile
     exponent and team size below 2^14 elements; from there the row-tile loop
-    (B = 12) with teams of 1 to 8 CTAs (on the B200, timed by whole OTOC
-    points, teams of 16 never won from 2^16 elements on: the cluster
-    barriers and the leader's expm cost more than the bandwidth they add)."""
+    (B = 12), and from 2^16 elements teams of 2 to 8 CTAs.  Timed by whole
+    OTOC points on the B200 (sparse SYK, 16-20 qubits), teams of 2 won at
+    every size; one CTA per problem took 1.7-1.8x longer (a problem's
+    vectors stream through one SM) and teams of 16 1.3x (their cluster
+    barriers and the leader CTA's expm cost more than the bandwidth they
+    add), so those two are not searched there."""
     if L < 14:
         return [(B, C) for B in range(8, min(12, L) + 1) for C in (1, 2, 4, 8, 16)
                 if C <= (1 << (L - B))]
-    teams = (1, 2, 4, 8, 16) if L < 16 else (1, 2, 4, 8)
+    teams = (1, 2, 4, 8, 16) if L < 16 else (2, 4, 8)
     return [(12, C) for C in teams if C <= (1 << (L - 12))]
 
 
