@@ -171,16 +171,20 @@ __device__ __noinline__ void team_dot(const Team &tm, const Cplx<float> *a, cons
 // run-time test inside the unrolled loads cost 15 % at every size.
 constexpr uint32_t STREAM_MIN = 1u << 17;
 template <bool STREAM>
-__device__ __forceinline__ Cplx<float> ld_basis(const Cplx<float> *p) {
+__device__ __forceinline__ float4 ld_basis(const Cplx<float> *p) {
     if constexpr (STREAM) {
-        const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
-        return Cplx<float>{v.x, v.y};
+        return __ldcs(reinterpret_cast<const float4 *>(p));
     } else {
-        return *p;
+        return *reinterpret_cast<const float4 *>(p);
     }
 }
 
-constexpr int TG = 8;   // basis vectors projected per pass over w
+constexpr int TG = 8;   // basis vectors projected (or added) per pass over w
+
+// The passes below move 16-byte packets (two complex64 elements) per load:
+// a team's range of every vector starts at an even element (ranges are
+// n / C elements, n >= 2^8, C <= 16) and the workspace vectors are 16-byte
+// aligned.  Each thread keeps up to TG + 1 packet loads in flight per step.
 
 // This thread's FP64 partial sums of <u_i|w>, i in [i0, i0 + ng).
 template <bool STREAM>
@@ -189,14 +193,21 @@ __device__ __forceinline__ void dots_pass(const Team &tm, Cplx<float> *const *u,
                                           double (&si)[TG]) {
 #pragma unroll
     for (int q = 0; q < TG; q++) sr[q] = si[q] = 0.0;
-    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
-        const Cplx<float> y = w[k];
+    const uint32_t lo = tm.lo(n) >> 1, hi = tm.hi(n) >> 1;
+    const float4 *w4 = reinterpret_cast<const float4 *>(w);
+    for (uint32_t k = lo + threadIdx.x; k < hi; k += BT) {
+        const float4 y = w4[k];
 #pragma unroll
         for (int q = 0; q < TG; q++) {
             if (q < ng) {
-                const Cplx<float> x = ld_basis<STREAM>(&u[i0 + q][k]);
-                sr[q] = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, sr[q]));
-                si[q] = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, si[q]));
+                const float4 x = ld_basis<STREAM>(&u[i0 + q][2 * k]);
+                double a = sr[q], b = si[q];
+                a = fma((double)x.x, (double)y.x, fma((double)x.y, (double)y.y, a));
+                b = fma((double)x.x, (double)y.y, fma(-(double)x.y, (double)y.x, b));
+                a = fma((double)x.z, (double)y.z, fma((double)x.w, (double)y.w, a));
+                b = fma((double)x.z, (double)y.w, fma(-(double)x.w, (double)y.z, b));
+                sr[q] = a;
+                si[q] = b;
             }
         }
     }
@@ -275,23 +286,35 @@ __device__ void team_string(const Team &tm, uint32_t x, uint32_t z, float cr, fl
     team_sync();
 }
 
-// This thread's share of w += sum_{i < nv} coef_i u_i; returns its part of ||w||^2.
+// This thread's share of w += sum_{i < nv} coef_i u_i; returns its part of
+// ||w||^2.  The basis vectors are read in groups of TG independent packet
+// loads (a run-time loop over single vectors left one load in flight).
 template <bool STREAM>
 __device__ __forceinline__ double axpy_pass(const Team &tm, Cplx<float> *const *u, const double *coef,
                                             int nv, Cplx<float> *w, uint32_t n) {
     double nrm = 0.0;
-    for (uint32_t k = tm.lo(n) + threadIdx.x; k < tm.hi(n); k += BT) {
-        const Cplx<float> w0 = w[k];
-        double xr = w0.x, xi = w0.y;
-        for (int i = 0; i < nv; i++) {
-            const Cplx<float> v = ld_basis<STREAM>(&u[i][k]);
-            const double cr = coef[2 * i], ci = coef[2 * i + 1];
-            xr = fma(cr, (double)v.x, fma(-ci, (double)v.y, xr));
-            xi = fma(cr, (double)v.y, fma(ci, (double)v.x, xi));
+    const uint32_t lo = tm.lo(n) >> 1, hi = tm.hi(n) >> 1;
+    float4 *w4 = reinterpret_cast<float4 *>(w);
+    for (uint32_t k = lo + threadIdx.x; k < hi; k += BT) {
+        const float4 w0 = w4[k];
+        double ar = w0.x, ai = w0.y, br = w0.z, bi = w0.w;
+        for (int i0 = 0; i0 < nv; i0 += TG) {
+#pragma unroll
+            for (int q = 0; q < TG; q++) {
+                if (i0 + q < nv) {
+                    const float4 v = ld_basis<STREAM>(&u[i0 + q][2 * k]);
+                    const double cr = coef[2 * (i0 + q)], ci = coef[2 * (i0 + q) + 1];
+                    ar = fma(cr, (double)v.x, fma(-ci, (double)v.y, ar));
+                    ai = fma(cr, (double)v.y, fma(ci, (double)v.x, ai));
+                    br = fma(cr, (double)v.z, fma(-ci, (double)v.w, br));
+                    bi = fma(cr, (double)v.w, fma(ci, (double)v.z, bi));
+                }
+            }
         }
-        const Cplx<float> r{(float)xr, (float)xi};
-        w[k] = r;
+        const float4 r = make_float4((float)ar, (float)ai, (float)br, (float)bi);
+        w4[k] = r;
         nrm = fma((double)r.x, (double)r.x, fma((double)r.y, (double)r.y, nrm));
+        nrm = fma((double)r.z, (double)r.z, fma((double)r.w, (double)r.w, nrm));
     }
     return nrm;
 }

@@ -69,8 +69,40 @@ __device__ __forceinline__ void row_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Rea
     }
 }
 
-// One term over a whole row: its source row from rq (see load_row), then
-// the case.
+// One term over one 16-byte chunk p of the row: w holds source chunk p ^ xq.
+template <typename Real, int K>
+__device__ __forceinline__ void chunk_term(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
+                                           const float4 &w, int p, Real c0, uint32_t jc) {
+    constexpr int EPC = 16 / (int)sizeof(Cplx<Real>);
+    constexpr int X0 = K & 1, Z0 = (K >> 1) & 1, KIND = K >> 2;
+    const Real cp = ((jc >> p) & 1u) ? -c0 : c0;
+#pragma unroll
+    for (int e = 0; e < EPC; e++) {
+        const int se = e ^ X0;
+        Real vx, vy;
+        if constexpr (EPC == 2) {
+            vx = se ? w.z : w.x;
+            vy = se ? w.w : w.y;
+        } else {
+            vx = __hiloint2double(__float_as_int(w.y), __float_as_int(w.x));
+            vy = __hiloint2double(__float_as_int(w.w), __float_as_int(w.z));
+        }
+        const Real c = (Z0 & se) ? -cp : cp;
+        Cplx<Real> &a = acc[EPC * p + e];
+        if (KIND == 0) {
+            a.x = fma(c, vx, a.x);
+            a.y = fma(c, vy, a.y);
+        } else {
+            a.x = fma(-c, vy, a.x);
+            a.y = fma(c, vx, a.y);
+        }
+    }
+}
+
+// One term over a whole row, its source row read from rq (see load_row)
+// one 16-byte chunk at a time, each applied as it arrives: 4 live load
+// registers per thread instead of 32, which keeps the kernel within the
+// register budget of two 288-thread CTAs per SM without spills.
 template <typename Real, int K>
 __device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<Real>)],
                                            uint32_t rq, Real c0, uint32_t jc) {
@@ -78,9 +110,14 @@ __device__ __forceinline__ void chunk_case(Cplx<Real> (&acc)[128 / sizeof(Cplx<R
     if constexpr (EPC == 1 && ((K & 1) || ((K >> 1) & 1))) {
         return;
     } else {
-        float4 w[8];
-        load_row(w, rq);
-        row_case<Real, K>(acc, w, c0, jc);
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            float4 w;
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(w.x), "=f"(w.y), "=f"(w.z), "=f"(w.w)
+                         : "r"(rq ^ ((uint32_t)p << 4)));
+            chunk_term<Real, K>(acc, w, p, c0, jc);
+        }
     }
 }
 

@@ -1,5 +1,5 @@
 """The failure path of the row kernel's pipeline waits, driven on the GPU
-without a fault (SURVEY's plan for device waits: a counter that never arrives).
+without a fault: a barrier whose expected copy never arrives.
 
 rp_test_withhold_tile makes the next row-kernel launch withhold one tile copy
 in its first CTA, so that CTA's consumers wait on a barrier that nothing
