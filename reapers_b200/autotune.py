@@ -133,8 +133,10 @@ def tune(problems, krydim=16, tol=1.2e-7, max_restarts=16, t_probe=0.3, sample=N
     for key, idx in by_key.items():
         if key not in cache:
             L = int(problems[idx[0]]["len"])
-            # enough problems to occupy every SM with teams of two or more CTAs
-            n = sample or min(len(idx), sms)
+            # the shape's own problems, up to two per SM: a class that needs a
+            # second wave of teams (168 problems on 148 two-CTA teams) must be
+            # timed with it, or its tail goes unseen
+            n = sample or min(len(idx), 2 * sms)
             base = [problems[j] for j in idx[:n]]
             timings = {}
             for B, C in candidates(L):
