@@ -32,6 +32,10 @@ Fixtures (numpy .npz):
                            4096 sampled indices plus the first and last, its
                            norm, and its projections onto 8 seeded random
                            vectors (a checksum of the whole state)
+  evolve_sparse_N48.npz    the same for the sparse SYK N = 48 evolve workload
+                           (24 qubits, k = 8, 384 terms, t = 10, m = 30, FP64),
+                           with 4 projections (an hour of the reference's CPU
+                           evolve on 8 threads)
 
 Usage: make_golden.py [name ...] regenerates only the named fixtures (file
 stems, e.g. dense_syk_N24_t10); without names, all of them.
@@ -50,6 +54,7 @@ import reapers_b200.syk as S  # noqa: E402
 
 
 N40_SEED, N40_PSI_SEED, N40_PROBE_SEED = 4040, 4041, 4042
+N48_SEED, N48_PSI_SEED, N48_PROBE_SEED = 4848, 4849, 4850
 
 
 def n40_problem():
@@ -65,6 +70,41 @@ def n40_problem():
     idx = np.unique(np.concatenate([[0, (1 << L) - 1],
                                     prng.integers(0, 1 << L, size=4096)])).astype(np.int64)
     return L, bits, coeff, psi, probes, idx
+
+
+def n48_problem():
+    """The 24-qubit evolve problem of evolve_sparse_N48.npz (the sparse SYK
+    N = 48 evolve workload: k = 8, 384 terms, m = 30, t = 10)."""
+    L = 24
+    bits, coeff = S.sparse_syk(48, k=8, seed=N48_SEED)
+    rng = np.random.default_rng(N48_PSI_SEED)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+    prng = np.random.default_rng(N48_PROBE_SEED)
+    idx = np.unique(np.concatenate([[0, (1 << L) - 1],
+                                    prng.integers(0, 1 << L, size=4096)])).astype(np.int64)
+    return L, bits, coeff, psi, prng, idx
+
+
+def probe_projections(prng, x, count=4):
+    """<r_c|x> for `count` seeded complex Gaussian vectors r_c, drawn one at
+    a time (a 24-qubit probe set would not fit in memory at once)."""
+    out = []
+    for _ in range(count):
+        r = prng.standard_normal(len(x)) + 1j * prng.standard_normal(len(x))
+        out.append(np.vdot(r, x))
+    return np.array(out)
+
+
+def make_sparse_n48(R):
+    L, bits, coeff, psi, prng, idx = n48_problem()
+    tol = float(np.finfo(np.float64).eps)
+    o, st = R.evolve(L, bits, coeff, psi, 10.0, 0.0, 30, tol)
+    np.savez_compressed(os.path.join(HERE, "evolve_sparse_N48.npz"), bits=bits, coeff=coeff,
+                        len=L, t=10.0, beta=0.0, krydim=30, tol=tol, idx=idx, vals=o[idx],
+                        norm=np.linalg.norm(o), proj=probe_projections(prng, o),
+                        applies=st["applies"], prods=st["prods"], ref_seconds=st["seconds"],
+                        seeds=np.array([N48_SEED, N48_PSI_SEED, N48_PROBE_SEED]))
 
 
 def make_dense_t10(R):
@@ -103,6 +143,8 @@ def main():
             make_dense_t10(R)
         if "evolve_sparse_N40" in only:
             make_sparse_n40(R)
+        if "evolve_sparse_N48" in only:
+            make_sparse_n48(R)
         return
     for N in range(4, 22, 2):
         L, b, c = R.majorana(N)
@@ -186,6 +228,7 @@ def main():
                         op_coeff=np.array([oc]), krydim=10, tol=1e-12)
     make_dense_t10(R)
     make_sparse_n40(R)
+    make_sparse_n48(R)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -153,3 +153,54 @@ def test_sparse_syk_n40_evolve_t10_reference_fixture(cuda):
           f"projections {err_proj:.2e}")
     assert err_rows < 1e-5 and err_proj < 1e-5
     hm.close()
+
+
+def test_sparse_syk_n48_evolve_t10_reference_fixture(cuda):
+    """Evolve parity on the sparse SYK N = 48 evolve workload itself (24
+    qubits, k = 8, 384 terms, t = 10, m = 30, tol = FP64 epsilon) against the
+    reference's own FP64 State::evolve: within 1e-12 on 4096 sampled entries
+    and on 4 projections of the whole state onto seeded random vectors,
+    identical H.psi and inner-product counts; the mixed path's error against
+    it is printed and bounded by 1e-5."""
+    path = os.path.join(GOLD, "evolve_sparse_N48.npz")
+    if not os.path.exists(path):
+        pytest.skip("evolve_sparse_N48.npz not generated")
+    g = np.load(path)
+    L = int(g["len"])
+    s_ham, s_psi, s_probe = (int(v) for v in g["seeds"])
+    bits, coeff = rb.syk.sparse_syk(48, k=8, seed=s_ham)
+    assert np.array_equal(bits, g["bits"]) and np.array_equal(coeff, g["coeff"])
+    rng = np.random.default_rng(s_psi)
+    psi = rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)
+    psi /= np.linalg.norm(psi)
+
+    def projections(x):
+        prng = np.random.default_rng(s_probe)
+        prng.integers(0, 1 << L, size=4096)     # the sampled indices come first
+        out = []
+        for _ in range(len(g["proj"])):
+            r = prng.standard_normal(1 << L) + 1j * prng.standard_normal(1 << L)
+            out.append(np.vdot(r, x))
+        return np.array(out)
+
+    ham = rb.Hamiltonian(L, bits, coeff, "c128")
+    x = dev(psi)
+    st = rb.evolve(ham, x, float(g["t"]), 0.0, int(g["krydim"]), float(g["tol"]))
+    o = x.cpu().numpy()
+    idx = g["idx"]
+    assert np.linalg.norm(o[idx] - g["vals"]) / np.linalg.norm(g["vals"]) < 1e-12
+    assert abs(np.linalg.norm(o) - float(g["norm"])) < 1e-12
+    assert np.abs(projections(o) - g["proj"]).max() < 1e-11 * np.abs(g["proj"]).max()
+    assert st["applies"] == int(g["applies"]) and st["prods"] == int(g["prods"])
+    ham.close()
+    hm = rb.Hamiltonian(L, bits, coeff, "c64")
+    xm = torch.empty(1 << L, dtype=torch.complex64, device=cuda)
+    rb.copy(xm, dev(psi))
+    rb.evolve(hm, xm, float(g["t"]), 0.0, int(g["krydim"]), float(np.finfo(np.float32).eps))
+    om = xm.cpu().numpy().astype(np.complex128)
+    err_rows = np.linalg.norm(om[idx] - g["vals"]) / np.linalg.norm(g["vals"])
+    err_proj = np.abs(projections(om) - g["proj"]).max() / np.abs(g["proj"]).max()
+    print(f"mixed vs reference FP64 at 24 qubits, t = 10: rows {err_rows:.2e}, "
+          f"projections {err_proj:.2e}")
+    assert err_rows < 1e-5 and err_proj < 1e-5
+    hm.close()
