@@ -885,9 +885,16 @@ def run_ours(args):
         del x, ham
         torch.cuda.empty_cache()
         sbits, scoeff = make_terms(cfg, seed=1000)
-        line["sharded_split_syk56"] = sharded_dist_leg(
-            SH.ProcessGroupComm(), L, sbits, scoeff, cfg["dtype"], steps=10, warmup=3,
-            make_state=lambda: rb.random_state(L, cfg["dtype"], seed=7, normalize=False))
+        # the value above is measured; a failure of this leg (e.g. no peer
+        # access between the GPUs) is recorded, not raised, so the line is
+        # still printed (a rank's failed collective ends by the process
+        # group's timeout on the others)
+        try:
+            line["sharded_split_syk56"] = sharded_dist_leg(
+                SH.ProcessGroupComm(), L, sbits, scoeff, cfg["dtype"], steps=10, warmup=3,
+                make_state=lambda: rb.random_state(L, cfg["dtype"], seed=7, normalize=False))
+        except Exception as e:   # noqa: BLE001 -- reported in the JSON line
+            line["sharded_split_syk56"] = {"failed": f"{type(e).__name__}: {e}"[:400]}
     # the single-GPU characterisation legs run only at N = 1 (under torchrun
     # every rank would repeat them while all GPUs are held)
     legs = world == 1
@@ -930,9 +937,14 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": os.cpu_count(),
                                     "kind": "reference", "sample": f"failed: {e}"}
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
+        if "failed" in line.get("sharded_split_syk56", {}):
+            # a collective of the failed leg may have left the communicator
+            # aborted: end without the teardown, which could wait on it
+            sys.stdout.flush()
+            os._exit(0)
         dist.destroy_process_group()
 
 
