@@ -293,6 +293,26 @@ def evolve_leg(seed=0, t=10.0, krydim=30, cpu=True):
     out["mixed_rel_err_vs_fp64"] = err
     out["speedup_mixed_vs_fp64"] = round(out["fp64_plain"]["seconds"] /
                                          out["mixed_fp32"]["seconds"], 3)
+    # the reference's own restarted Krylov on its own GPU backend (GPUImpl,
+    # cuBLAS BLAS-1 and krnl_apply_ops, built for sm_100a), same Hamiltonian,
+    # t, m and tol, from its own random state
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_driver")
+    if os.path.exists(drv):
+        from oracle import oracle as O
+        tf = os.path.join(tempfile.mkdtemp(prefix="rpgpu_"), "terms")
+        O.write_terms(tf, L, bits, coeff)
+        r = subprocess.run([drv, "evolve", tf, "64", repr(float(t)), str(krydim),
+                            repr(float(np.finfo(np.float64).eps))],
+                           capture_output=True, text=True, timeout=900)
+        if r.returncode == 0:
+            g = json.loads(r.stdout.strip().splitlines()[-1])
+            out["reference_gpu_evolve"] = {
+                "seconds": g["seconds"], "applies": g["applies"],
+                "what": "the reference's State::evolve on its GPUImpl backend, sm_100a build"}
+            out["speedup_fp64_vs_reference_gpu"] = round(g["seconds"] /
+                                                          out["fp64_plain"]["seconds"], 1)
+        else:
+            out["reference_gpu_evolve"] = {"failed": r.stderr[-300:]}
     if cpu:
         try:
             rows = 1 << 18

@@ -17,6 +17,12 @@
 //   ref_gpu_driver bench terms fp reps      ms per GPUImpl::apply_ops on a
 //                                           random state (CUDA events, after one
 //                                           warm-up apply), as JSON
+//   ref_gpu_driver evolve terms fp t krydim tol
+//                                           the reference's restarted Krylov
+//                                           (State::evolve, inc/algo.h:267-365)
+//                                           on its GPU backend from a random
+//                                           state: seconds and H.psi count, JSON
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -27,6 +33,18 @@
 using namespace REAPERS;
 
 #include "ref_io.h"
+
+// GPUImpl with an H.psi counter, as ref_driver.cc's CountingImpl does for
+// the CPU backend.
+struct CountingGPU : GPUImpl {
+    static inline long n_apply = 0;
+    template <RealScalar FpType>
+    static void apply_ops(typename SpinOp<FpType>::IndexType len, BufType<FpType> res,
+                          const DevSumOps<FpType> &ops, ConstBufType<FpType> vec) {
+        n_apply++;
+        GPUImpl::apply_ops(len, res, ops, vec);
+    }
+};
 
 // the reference's GPU Hamiltonian (DevSumOps) from the stored terms
 template <typename Fp>
@@ -63,6 +81,24 @@ static int run(int argc, char **argv, const std::string &mode, const std::vector
         }
         return 0;
     }
+    if (mode == "evolve") {
+        const double t = std::atof(argv[4]);
+        const int krydim = std::atoi(argv[5]);
+        const double tol = std::atof(argv[6]);
+        State<Fp, CountingGPU> x(len);
+        x.random_state();
+        State<Fp, CountingGPU> w(x);
+        w.evolve(ops, 0.01, 0.0, krydim, (Fp)tol);   // warm-up: uploads, buffers
+        CountingGPU::n_apply = 0;
+        cudaDeviceSynchronize();
+        const auto t0 = std::chrono::steady_clock::now();
+        x.evolve(ops, t, 0.0, krydim, (Fp)tol);
+        cudaDeviceSynchronize();
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("{\"seconds\": %.4f, \"applies\": %ld, \"len\": %d, \"fp\": %d}\n", sec,
+                    CountingGPU::n_apply, len, (int)(8 * sizeof(Fp)));
+        return 0;
+    }
     const int reps = std::atoi(argv[4]);
     GSt x(len), y(len);
     x.random_state();
@@ -84,13 +120,13 @@ static int run(int argc, char **argv, const std::string &mode, const std::vector
 
 int main(int argc, char **argv) {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: ref_gpu_driver apply|bench terms fp vec out | reps\n");
+        std::fprintf(stderr, "usage: ref_gpu_driver apply|bench|evolve terms fp ...\n");
         return 1;
     }
     const std::string mode = argv[1];
     int len = 0;
     const auto terms = read_terms(argv[2], len);
     const int fp = std::atoi(argv[3]);
-    if (mode != "apply" && mode != "bench") return 1;
+    if (mode != "apply" && mode != "bench" && mode != "evolve") return 1;
     return fp == 64 ? run<double>(argc, argv, mode, terms, len) : run<float>(argc, argv, mode, terms, len);
 }
