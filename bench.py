@@ -213,7 +213,7 @@ def otoc_leg(cfg, bits, coeff, seed, npts=2, krydim=16, last=True):
     return out
 
 
-def otoc_full_leg(cfg, nreal, nstates, krydim=16, npts=20, seed0=1000, first=0):
+def otoc_full_leg(cfg, nreal, nstates, krydim=16, npts=20, seed0=1000, first=0, first_state=0):
     """The N = 56 OTOC workload as stated: nreal disorder realisations x
     nstates random states, F(t) at all `npts` points of the grid on [0, 15],
     m = 16, in the plain FP64 path and the mixed path, through otoc_leg's
@@ -228,7 +228,7 @@ def otoc_full_leg(cfg, nreal, nstates, krydim=16, npts=20, seed0=1000, first=0):
     err = 0.0
     for r in range(first, first + nreal):
         bits, coeff = rb.syk.sparse_syk(cfg["N"], k=cfg["k"], seed=seed0 + r)
-        for st in range(nstates):
+        for st in range(first_state, first_state + nstates):
             leg = otoc_leg(cfg, bits, coeff, seed=7 + 31 * r + st, npts=npts - 1, krydim=krydim,
                            last=False)
             for k in tot:
@@ -935,7 +935,8 @@ def run_ours(args):
     if legs and args.config == "syk56" and args.otoc_full:
         spec, _, first = args.otoc_full.partition("+")
         nr, ns = (int(v) for v in spec.split("x"))
-        line["otoc_full"] = otoc_full_leg(cfg, nr, ns, first=int(first or 0))
+        line["otoc_full"] = otoc_full_leg(cfg, nr, ns, first=int(first or 0),
+                                          first_state=args.otoc_first_state)
     if legs and args.config == "syk56" and not args.no_evolve:
         line["evolve_syk48"] = evolve_leg(seed=rank, cpu=(rank == 0 and world == 1 and not args.no_cpu))
     if legs and args.config == "syk56" and not args.no_batch:
@@ -1052,6 +1053,8 @@ def main():
                     help="RxS[+F]: also run the N = 56 OTOC on R realisations (from number F, "
                          "default 0) x S states at all 20 points in both precisions (e.g. 4x2; "
                          "minutes per problem)")
+    ap.add_argument("--otoc-first-state", type=int, default=0,
+                    help="first random state of --otoc-full (states first .. first + S - 1)")
     ap.add_argument("--profile", action="store_true",
                     help="run two applies and exit (for an ncu capture)")
     args = ap.parse_args()
