@@ -282,7 +282,10 @@ public:
     B200SumOps(const SpinOp<FpType> &op) : HostSumOps<FpType>(op) {}
     B200SumOps(const HostSumOps<FpType> &ops) : HostSumOps<FpType>(ops) {}
     B200SumOps(const B200SumOps &ops) : HostSumOps<FpType>(ops) {}
-    B200SumOps(B200SumOps &&ops) : HostSumOps<FpType>(std::move(ops)) {}
+    /* The reference's HostSumOps moves its term list without a release();
+     * the device tables built for a list stay with neither object, so both
+     * sides rebuild them on their next use. */
+    B200SumOps(B200SumOps &&ops) : HostSumOps<FpType>(std::move(ops)) { ops.drop(); }
     template <RealScalar FpType1>
     explicit B200SumOps(const B200SumOps<FpType1> &ops) : HostSumOps<FpType>(ops) {}
     B200SumOps(const std::initializer_list<SpinOp<FpType>> &l = {}) : HostSumOps<FpType>(l) {}
@@ -292,7 +295,11 @@ public:
         return *this;
     }
     B200SumOps &operator=(B200SumOps &&rhs) {
-        if (this != &rhs) HostSumOps<FpType>::operator=(static_cast<HostSumOps<FpType> &&>(rhs));
+        if (this != &rhs) {
+            drop();
+            rhs.drop();
+            HostSumOps<FpType>::operator=(static_cast<HostSumOps<FpType> &&>(rhs));
+        }
         return *this;
     }
     ~B200SumOps() { drop(); }

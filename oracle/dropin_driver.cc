@@ -140,6 +140,20 @@ int main(int argc, char **argv) {
     const auto Fg = g0 * pg;
     const double otoc = std::abs(Fg - Fc) / std::abs(c0 * c0);
 
+    // a moved operator keeps no device table of its old term list: apply
+    // one, move-assign another onto it, apply again
+    double moved = 0.0;
+    {
+        B200SumOps<double> a(ham_g), b(SpinOp<double>::sigma_z(0));
+        GSt t1 = a * g0;
+        (void)t1;
+        a = std::move(b);
+        GSt t2 = a * g0;
+        CSt z0(c0);
+        z0 *= HostSumOps<double>(SpinOp<double>::sigma_z(0));
+        moved = rel_diff(t2, z0);
+    }
+
     // changing the operator drops its device table (release()); the next
     // apply uploads the new term list
     ham_c += SpinOp<double>::sigma_x(0) * SpinOp<double>::sigma_y(1);
@@ -253,8 +267,9 @@ int main(int argc, char **argv) {
         "\"N\": %d, \"terms\": %zu, \"term_diff\": %.3e, \"roundtrip\": %.3e, \"elem\": %.3e, "
         "\"apply\": %.3e, \"evolve_ref_krylov\": %.3e, \"evolve_b200krylov\": %.3e, "
         "\"evolve_beta\": %.3e, \"otoc\": %.3e, \"F\": [%.12e, %.12e], \"mutate\": %.3e, "
+        "\"moved\": %.3e, "
         "\"E0_cpu\": %.15e, \"E0_b200\": %.15e, \"ground_overlap\": %.15f}\n",
         N, ham_c.size(), terms, roundtrip, elem, apply, evolve, evolve_fused, evolve_beta, otoc,
-        (double)Fc.real(), (double)Fc.imag(), mutate, Ec, Eg, overlap);
+        (double)Fc.real(), (double)Fc.imag(), mutate, moved, Ec, Eg, overlap);
     return 0;
 }

@@ -8,7 +8,8 @@ the SYK term list, the host->device->host state round trip, element access,
 State operator* (H.psi), the reference's restarted Krylov evolve, the
 GPU-resident Krylov selected as State::evolve<B200Krylov>, imaginary-time
 evolution, the OTOC sequence of examples/simple-syk-krylov.cc, an apply
-after the operator is changed (device table dropped and rebuilt), and the
+after the operator is changed (device table dropped and rebuilt) or
+move-assigned from another (no stale table of the old terms), and the
 reference's ground-state Lanczos (energy; state overlap where the ground
 state is not degenerate); the reference's exact diagonalisation
 (ExactDiagonalization: eigensystem, matexp cache, mat_mul and the
@@ -48,7 +49,7 @@ def test_reference_code_on_b200impl_matches_cpuimpl(N, sp, seed, t, krydim):
     d = json.loads(r.stdout.strip().splitlines()[-1])
     assert d["term_diff"] == 0.0
     assert d["roundtrip"] == 0.0 and d["elem"] == 0.0
-    for k in ("apply", "evolve_ref_krylov", "evolve_b200krylov", "evolve_beta", "mutate"):
+    for k in ("apply", "evolve_ref_krylov", "evolve_b200krylov", "evolve_beta", "mutate", "moved"):
         assert d[k] <= 1e-12, (k, d)
     assert d["otoc"] <= 1e-11, d
     # parity-block form: block gen_ham, the examples/syk.cc OTOC on one block,
