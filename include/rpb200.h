@@ -238,7 +238,7 @@ int rp_dense_expm(rp_dense_t d, double cr, double ci, void *out);
 int rp_dense_destroy(rp_dense_t d);
 /* res = mat vec for a dense dim x dim column-major device matrix
  * (GPUImpl::mat_mul, inc/gpuimpl.h:1012-1021): FP64 accumulation, fixed
- * summation order; res and vec distinct. */
+ * summation order; res and vec distinct; dim at most 2^16. */
 int rp_mat_vec(int dtype, uint64_t dim, const void *mat, const void *vec, void *res);
 
 /* --- time-stepped Krylov primitives (no reference counterpart: the

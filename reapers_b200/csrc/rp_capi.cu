@@ -836,6 +836,7 @@ int rp_mat_vec(int dtype, uint64_t dim, const void *mat, const void *vec, void *
         check_vec(vec);
         check_vec(res);
         RP_REQUIRE(res != vec, RP_E_INVALID, "mat_vec needs distinct input and output vectors");
+        RP_REQUIRE(dim <= (1ull << 16), RP_E_INVALID, "mat_vec takes matrices of at most 2^16 rows");
         dense_matvec(dtype, dim, mat, vec, res, g_stream);
     });
 }

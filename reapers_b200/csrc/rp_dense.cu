@@ -165,12 +165,12 @@ void dense_build(DenseSystem &d, int len, int dtype, const uint64_t *bits, const
     }
     ensure_handles(st);
     const size_t mbytes = dim * dim * esz(dtype);
-    RP_CUDA(cudaMalloc(&d.evecs, mbytes));
-    RP_CUDA(cudaMalloc(&d.evals_dev, dim * sizeof(double)));
     DenseTerm *dterms = nullptr;
     int *info = nullptr;
     void *work = nullptr;
     try {
+        RP_CUDA(cudaMalloc(&d.evecs, mbytes));
+        RP_CUDA(cudaMalloc(&d.evals_dev, dim * sizeof(double)));
         RP_CUDA(cudaMalloc((void **)&dterms, std::max<size_t>(1, terms.size()) * sizeof(DenseTerm)));
         RP_CUDA(cudaMalloc((void **)&info, sizeof(int)));
         if (!terms.empty())

@@ -106,6 +106,9 @@ class DenseEvolver:
         """psi <- exp(-(beta + i t) H) psi in place (ExactDiagonalization::evolve)."""
         import torch
         from . import _lib, _ptr, _tcode
+        if psi.dtype != self.dtype or psi.numel() != 1 << self.ham.len:
+            raise ValueError(f"state must be {self.dtype} of length {1 << self.ham.len}, "
+                             f"got {psi.dtype} of length {psi.numel()}")
         if t == 0.0 and beta == 0.0:
             return psi
         E = self.matexp(complex(-beta, -t))
