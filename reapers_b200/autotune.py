@@ -50,12 +50,18 @@ def _load():
 
 
 def _save(d):
+    """Write the cache; an unwritable location only costs the next batch a
+    new search, so it is not an error."""
     p = cache_path()
-    os.makedirs(os.path.dirname(p), exist_ok=True)
-    tmp = p + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(d, f, indent=1, sort_keys=True)
-    os.replace(tmp, p)
+    try:
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        tmp = p + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, p)
+        return True
+    except OSError:
+        return False
 
 
 def shape_key(prob, krydim):

@@ -33,3 +33,17 @@ def test_shape_key_groups_realisations_by_size_and_group_count():
     assert AT.shape_key({"len": 16, "bits": bits}, 16).startswith("L16-")
     g = len(np.unique(S.xmask(bits) >> np.uint64(11)))
     assert AT.shape_key({"len": 16, "bits": bits}, 12) == f"L16-G{32 * round(g / 32)}-c64-m12-p"
+
+
+def test_cache_round_trip_and_unwritable_location(tmp_path, monkeypatch):
+    monkeypatch.setenv("RPB200_TUNE_CACHE", str(tmp_path / "sub" / "tune.json"))
+    rec = {"L20-G64-c64-m16-p": {"path": "batched", "tile": 12, "team": 2}}
+    assert AT._save(rec)
+    assert AT._load() == rec
+    # a path under a regular file cannot be created: the save reports it and
+    # the load falls back to an empty cache instead of raising
+    blocker = tmp_path / "file"
+    blocker.write_text("x")
+    monkeypatch.setenv("RPB200_TUNE_CACHE", str(blocker / "tune.json"))
+    assert AT._save(rec) is False
+    assert AT._load() == {}
