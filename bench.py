@@ -315,14 +315,14 @@ def evolve_leg(seed=0, t=10.0, krydim=30, cpu=True):
             out["reference_gpu_evolve"] = {"failed": r.stderr[-300:]}
     if cpu:
         try:
-            rows = 1 << 18
-            cb = cpu_reference(cfg, bits, coeff, 0.0, rows, 1)
-            per_apply = cb["seconds"] * ((1 << L) / rows)
+            cb = cpu_sample(cfg, bits, coeff, 0.0, 1 << 18)
+            per_apply = cb["seconds"] * ((1 << L) / cb["rows"])
             est = per_apply * out["fp64_plain"]["applies"]
             out["cpu_reference_estimate"] = {
                 "seconds_lower_bound": round(est, 2), "cores": cb["threads"],
-                "sample": f"reference SpinOp::apply over {rows} of 2^{L} rows: "
-                          f"{per_apply:.3f} s per H.psi x {out['fp64_plain']['applies']} H.psi"}
+                "kind": cb["kind"],
+                "sample": f"{cb['sample']}: {per_apply:.3f} s per H.psi x "
+                          f"{out['fp64_plain']['applies']} H.psi"}
             out["speedup_fp64_vs_cpu_estimate"] = round(est / out["fp64_plain"]["seconds"], 1)
         except Exception as e:   # a reported baseline only
             out["cpu_reference_estimate"] = {"failed": str(e)}
@@ -749,6 +749,58 @@ def cpu_reference(cfg, bits, coeff, alg_bytes, rows, reps):
             "threads": d["threads"], "rows": rows, "isa": isa}
 
 
+PORT_ROWS = 1 << 15   # output rows per timed sample of the oracle's port
+
+
+def port_state(cfg, seed=7):
+    """A random state of the workload's size and precision, resident in host
+    memory, for the port's timed samples."""
+    L = cfg["N"] // 2
+    real = np.float32 if cfg["dtype"] == "c64" else np.float64
+    v = np.random.default_rng(seed).standard_normal(2 << L, dtype=real)
+    return v.view(np.complex64 if real is np.float32 else np.complex128)
+
+
+def port_reference(cfg, bits, coeff, alg_bytes, rows, state):
+    """Time the oracle's restatement of the reference CPU apply (SpinOp::apply
+    summed over the terms in list order, inc/ops.h:421-440, as looped by
+    CPUImpl::apply_ops, inc/cpuimpl.h:739-754) on the first `rows` output rows
+    of `state`: the stand-in for the reference build where oracle/_ref was not
+    built.  numpy, one host thread."""
+    from oracle import oracle as O
+    L = cfg["N"] // 2
+    idx = np.arange(rows, dtype=np.uint64)
+    t0 = time.perf_counter()
+    O.apply_at(bits, coeff, idx, lambda j: state[j])
+    dt = time.perf_counter() - t0
+    return {"value": alg_bytes * (rows / (1 << L)) / dt / 1e9, "seconds": dt, "threads": 1,
+            "rows": rows, "isa": "numpy"}
+
+
+def cpu_sample(cfg, bits, coeff, alg_bytes, rows, state=None):
+    """One timed sample of the reference's CPU apply over `rows` output rows:
+    the reference build (oracle/_ref) where it was built, else the oracle's
+    port over min(rows, PORT_ROWS) rows of `state` (port_state(cfg) when
+    None).  Returns the timing with its 'kind' and a one-line 'sample'."""
+    from oracle import oracle as O
+    L = cfg["N"] // 2
+    if O.ref_available():
+        cb = cpu_reference(cfg, bits, coeff, alg_bytes, rows, 1)
+        cb["kind"] = "reference"
+        cb["sample"] = (f"reference SpinOp::apply (CPUImpl::apply_ops loop) over {rows} of "
+                        f"2^{L} output rows, same terms, OpenMP {cb['threads']} threads "
+                        f"({cb['isa']} build)")
+    else:
+        prow = min(rows, PORT_ROWS, 1 << L)
+        cb = port_reference(cfg, bits, coeff, alg_bytes, prow,
+                            port_state(cfg) if state is None else state)
+        cb["kind"] = "port"
+        cb["sample"] = (f"the oracle's restatement of SpinOp::apply over {prow} of 2^{L} "
+                        f"output rows, same terms, numpy, 1 thread (the reference build "
+                        f"oracle/_ref was absent)")
+    return cb
+
+
 def dist_setup(n):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -946,15 +998,13 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = 1 << 20 if cfg["N"] >= 56 else 1 << 18
         try:
-            cb = cpu_reference(cfg, bits, coeff, alg_dram, rows, 1)
+            cb = cpu_sample(cfg, bits, coeff, alg_dram, rows)
             line["cpu_baseline"] = {"value": round(cb["value"], 4), "unit": "GB/s",
-                                    "cores": cb["threads"], "kind": "reference",
-                                    "sample": f"reference SpinOp::apply over {rows} of 2^{L} "
-                                              f"output rows, same terms, OpenMP "
-                                              f"{cb['threads']} threads ({cb['isa']} build), "
-                                              f"{cb['seconds']:.2f} s; value = the whole "
-                                              f"apply's HBM bytes x the row fraction / time "
-                                              f"(extrapolated from the sample)"}
+                                    "cores": cb["threads"], "kind": cb["kind"],
+                                    "sample": f"{cb['sample']}, {cb['seconds']:.2f} s; value "
+                                              f"= the whole apply's HBM bytes x the row "
+                                              f"fraction / time (extrapolated from the "
+                                              f"sample)"}
         except Exception as e:   # the baseline is reported, never the target
             line["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": os.cpu_count(),
                                     "kind": "reference", "sample": f"failed: {e}"}
@@ -976,27 +1026,22 @@ def run_reference(args):
     if rank != 0:
         return
     from oracle import oracle as O
-    if not O.ref_available():
-        print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref/ref_driver was not built"}))
-        return
     L = cfg["N"] // 2
     bits, coeff = make_terms(cfg, seed=1000)
     # the bytes are those of our arm's plan (host-side grouping), so both arms
     # report the same unit for the same work
     alg = alg_bytes_host(L, bits, cfg["dtype"])
     rows = 1 << 19 if cfg["N"] >= 56 else 1 << 17
+    state = None if O.ref_available() else port_state(cfg)
     times = []
     for i in range(args.warmup + args.steps):
-        cb = cpu_reference(cfg, bits, coeff, alg, rows, 1)
+        cb = cpu_sample(cfg, bits, coeff, alg, rows, state)
         if i >= args.warmup:
             times.append(cb["seconds"])
     t = float(np.mean(times))
-    value = alg * (rows / (1 << L)) / t / 1e9
-    sample = (f"reference SpinOp::apply (CPUImpl::apply_ops loop) over {rows} of 2^{L} output "
-              f"rows per step, OpenMP {cb['threads']} threads ({cb['isa']} build); value = the "
-              f"whole apply's HBM bytes x the row fraction / time, i.e. extrapolated from the "
-              f"row sample")
+    value = alg * (cb["rows"] / (1 << L)) / t / 1e9
+    sample = (f"{cb['sample']} per step; value = the whole apply's HBM bytes x the row "
+              f"fraction / time, i.e. extrapolated from the row sample")
     line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "impl": "reference",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
@@ -1006,7 +1051,7 @@ def run_reference(args):
             "config": {"workload": cfg["workload"], "sample": sample,
                        "value_is": "extrapolated from a row sample"},
             "cpu_baseline": {"value": round(value, 4), "unit": "GB/s",
-                             "cores": cb["threads"], "kind": "reference", "sample": sample},
+                             "cores": cb["threads"], "kind": cb["kind"], "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -1019,7 +1064,7 @@ def alg_bytes_host(L, bits, dtype, sms=148):
     CTAs, G_w = distinct x >> (B + floor(log2 window))."""
     import reapers_b200.syk as S
     B = 12 if dtype == "c64" else 11
-    win = min(1 << (L - B), 2 * sms)
+    win = min(1 << max(L - B, 0), 2 * sms)
     lw = 0
     while (2 << lw) <= win:
         lw += 1

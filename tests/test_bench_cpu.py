@@ -36,3 +36,41 @@ def test_compulsory_bytes_window_follows_the_tile_count():
     small = bench.alg_bytes_host(19, bits & np.uint64((1 << 38) - 1), "c64", sms=148)
     gw_small = len(np.unique(S.xmask(bits & np.uint64((1 << 38) - 1)) >> np.uint64(12 + 7)))
     assert small == (gw_small + 1) * (1 << 19) * 8
+
+
+SMALL = dict(N=28, k=8, dtype="c64", workload="sparse SYK N=28 (14 qubits), k=8")
+
+
+def test_port_sample_computes_the_apply_it_times(monkeypatch):
+    """Where the reference build is absent the CPU baseline times the
+    oracle's port on a row sample; the rows it computes are those of the
+    full oracle apply, and the rate is extrapolated from the sample."""
+    from oracle import oracle as O
+    monkeypatch.setattr(O, "ref_available", lambda: False)
+    bits, coeff = bench.make_terms(SMALL, seed=3)
+    state = bench.port_state(SMALL)
+    assert state.dtype == np.complex64 and state.size == 1 << 14
+    cb = bench.cpu_sample(SMALL, bits, coeff, 1e9, 1 << 18, state)
+    assert cb["kind"] == "port" and cb["threads"] == 1
+    assert cb["rows"] == 1 << 14             # the whole state when it is smaller
+    assert cb["value"] == 1e9 * 1.0 / cb["seconds"] / 1e9
+    idx = np.arange(100, dtype=np.uint64)
+    full = O.apply(14, bits, coeff, state.astype(np.complex128))
+    part = O.apply_at(bits, coeff, idx, lambda j: state[j])
+    np.testing.assert_allclose(part, full[:100], rtol=1e-12, atol=1e-12)
+
+
+def test_reference_arm_falls_back_to_the_port(monkeypatch, capsys):
+    import json
+    from oracle import oracle as O
+    monkeypatch.setattr(O, "ref_available", lambda: False)
+    monkeypatch.setitem(bench.CONFIGS, "small", SMALL)
+    monkeypatch.delenv("RANK", raising=False)
+    args = bench.argparse.Namespace(config="small", steps=2, warmup=1)
+    bench.run_reference(args)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" not in line
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 1
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 == line["e2e"]["d2h_bytes_per_step"]
+    assert line["config"]["value_is"] == "extrapolated from a row sample"
