@@ -74,3 +74,11 @@ def test_reference_arm_falls_back_to_the_port(monkeypatch, capsys):
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 == line["e2e"]["d2h_bytes_per_step"]
     assert line["config"]["value_is"] == "extrapolated from a row sample"
+
+
+def test_compulsory_bytes_of_a_state_smaller_than_one_tile():
+    """Below one tile (2^12 complex64 elements) the window is the one tile:
+    G_w counts distinct x >> 12 and the formula stays (G_w + 1) * D * 8."""
+    bits, _ = S.sparse_syk(20, k=8, seed=3)
+    gw = len(np.unique(S.xmask(bits) >> np.uint64(12)))
+    assert bench.alg_bytes_host(10, bits, "c64") == (gw + 1) * (1 << 10) * 8
