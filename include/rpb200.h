@@ -123,7 +123,8 @@ int rp_vec_dot(int dtype, uint64_t n, const void *a, const void *b, double *out)
  * cudaMalloc / cudaFree would implicitly synchronise the device).  No
  * counterpart in the reference.  Its scratch is a fixed 16 KB device array
  * (up to 1024 per-block partial sums); n may be at most 2^28 (larger n
- * returns RP_E_INVALID with a message).
+ * returns RP_E_INVALID with a message); a and b 16-byte aligned, as for
+ * every vector entry point.
  * The first call on each device looks up the array's device address; make
  * that first call before any stream capture.  All calls share the array:
  * calls that overlap on the GPU race.  Runs on the legacy default stream. */

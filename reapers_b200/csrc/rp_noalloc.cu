@@ -95,6 +95,8 @@ extern "C" int rp_vec_dot_noalloc(int dtype, uint64_t n, const void *a, const vo
         RP_REQUIRE(dtype == RP_C64 || dtype == RP_C128, RP_E_INVALID,
                    "dtype must be RP_C64 (1) or RP_C128 (2)");
         RP_REQUIRE(a && b && out, RP_E_INVALID, "null pointer");
+        RP_REQUIRE((((uintptr_t)a | (uintptr_t)b) & 15) == 0, RP_E_INVALID,
+                   "vectors must be 16-byte aligned");
         RP_REQUIRE(n <= NOALLOC_MAX_ELEMS, RP_E_INVALID,
                    "rp_vec_dot_noalloc: vector length " + std::to_string(n) +
                        " exceeds the fixed scratch limit of " + std::to_string(NOALLOC_MAX_ELEMS) +

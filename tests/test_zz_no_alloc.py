@@ -61,3 +61,20 @@ def test_noalloc_dot_rejects_too_long_vectors():
                                 C.c_void_p(a.data_ptr()), out)
     assert rc == -2
     assert b"exceeds the fixed scratch limit" in lib.rp_last_error()
+
+
+def test_noalloc_dot_rejects_misaligned_vectors():
+    """A vector that starts off a 16-byte boundary is refused before any
+    launch, as by every other vector entry point."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import reapers_b200 as rb
+    from reapers_b200 import _lib
+    rb.init(0)
+    lib = _lib.load()
+    a = torch.zeros(64, dtype=torch.complex64, device="cuda")
+    out = (C.c_double * 2)()
+    rc = lib.rp_vec_dot_noalloc(1, 8, C.c_void_p(a.data_ptr() + 8), C.c_void_p(a.data_ptr()), out)
+    assert rc == -2
+    assert b"16-byte aligned" in lib.rp_last_error()
