@@ -1,9 +1,10 @@
 """Edges of the restarted Krylov evolve (Krylov<Impl>::evolve,
 inc/algo.h:267-365) against the oracle, FP64: the smallest and largest basis
 sizes, a start vector that is an eigenvector (breakdown on the first basis
-vector), an empty Hamiltonian, and pure imaginary time.  The final state
-within 1e-12 relative; restart, H.psi, pass and inner-product counts and the
-breakdown flag identical."""
+vector), an empty Hamiltonian, and pure imaginary time.  FP64: the final
+state within 1e-12 relative; restart, H.psi, pass and inner-product counts
+and the breakdown flag identical.  Mixed path (complex64 vectors, FP64
+Krylov internals): within 1e-5 relative of the FP64 oracle."""
 import numpy as np
 import pytest
 import torch
@@ -68,3 +69,32 @@ def test_pure_imaginary_time(cuda):
     bits, coeff = rb.syk.sparse_syk(2 * L, k=4, seed=10)
     got, _ = _run(bits, coeff, _start(), 0.0, 0.7, 8)
     assert np.linalg.norm(got) > 1.0      # exp(-beta H) is not unitary
+
+
+def _run_mixed(bits, coeff, v, t, beta, m):
+    """The mixed path (complex64 vectors, FP64 Krylov internals) against the
+    FP64 oracle, to the path's FP32 tolerance."""
+    ham = rb.Hamiltonian(L, bits, coeff, "c64")
+    x = torch.from_numpy(np.ascontiguousarray(v)).to(torch.complex64).cuda()
+    st = rb.evolve(ham, x, t, beta, m, float(np.finfo(np.float32).eps))
+    got = x.cpu().numpy().astype(np.complex128)
+    ham.close()
+    ref, _ = O.evolve(L, bits, coeff, v.astype(np.complex64).astype(np.complex128), t, beta, m,
+                      1e-12)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+    return got, st
+
+
+@pytest.mark.parametrize("m", [2, 64])
+def test_mixed_smallest_and_largest_basis(cuda, m):
+    bits, coeff = rb.syk.sparse_syk(2 * L, k=4, seed=10)
+    _run_mixed(bits, coeff, _start(), 1.0, 0.0, m)
+
+
+def test_mixed_empty_hamiltonian_and_imaginary_time(cuda):
+    v = _start()
+    got, st = _run_mixed(np.zeros(0, np.uint64), np.zeros(0, np.complex128), v, 0.9, 0.0, 6)
+    assert st["breakdown"] == 1
+    assert np.array_equal(got, v.astype(np.complex64).astype(np.complex128))
+    bits, coeff = rb.syk.sparse_syk(2 * L, k=4, seed=10)
+    _run_mixed(bits, coeff, v, 0.0, 0.7, 8)
